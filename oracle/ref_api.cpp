@@ -1,0 +1,185 @@
+// ref_api.cpp -- C entry points around the reference's own fill and verify programs
+// (TEST INFRASTRUCTURE ONLY: linked into oracle/_ref/libbpmax_ref.so with the reference
+// TPDS V3 objects compiled from their sources; used to pin the oracle, to generate the golden
+// fixtures and as the timed CPU baseline).
+//
+//  ref_bpmax_fill   -> void bpmax(long M,long N,long N_sec,long N_tile,long R,long MR,long NR,
+//                                 long P,int* seq1,int* seq2,float****** FTable)  (V3/bpmax.c:129)
+//  ref_bpmax_verify -> void bpmax_verify(long M,long N,int*,int*,float**** FTable)
+//                                                                      (V3/bpmax_verify.c:156)
+//
+// The pointer trees are built over caller buffers exactly as the reference's CLI wrapper does
+// (V3/bpmax-wrapper.c:175-197 and :198-213). icpc, which the reference Makefile uses, runs with
+// flush-to-zero and denormals-are-zero; the reference is only self-consistent in that mode
+// (its seeds 1.401298464324817E-45 in V3/bpmax_inner_reductions_finalize.c:141-142 would
+// otherwise survive into +0 cells), so every OpenMP thread gets FTZ|DAZ for the call and its
+// previous MXCSR back afterwards. The reference prints progress lines to stdout; they are
+// sent to /dev/null so callers keep a clean stdout.
+//
+// The optimised fill reads parts of its own scratch buffers (allocated with malloc/_mm_malloc
+// in V3/bpmax.c:148-250 and V3/bpmax_inner_reductions_finalize.c:127-131, never cleared)
+// before writing them. Its result is right when that memory is zero, as fresh mmap pages of
+// large allocations are, and wrong (heap garbage such as 2.4e-38 or 3.5e20 in logical cells,
+// varying with thread count) when the heap recycles dirty chunks. With zero_scratch=1 glibc's
+// M_PERTURB makes every allocation during the call start at zero, which reproduces the
+// large-size behaviour at every size; the reference sources stay unchanged.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fcntl.h>
+#include <malloc.h>
+#include <omp.h>
+#include <unistd.h>
+#include <xmmintrin.h>
+
+void bpmax(long, long, long, long, long, long, long, long, int *, int *, float ******);
+void bpmax_verify(long, long, int *, int *, float ****);
+
+namespace {
+
+struct QuietStdout {
+    int saved = -1;
+    QuietStdout()
+    {
+        fflush(stdout);
+        saved = dup(1);
+        int devnull = open("/dev/null", O_WRONLY);
+        if (devnull >= 0) { dup2(devnull, 1); close(devnull); }
+    }
+    ~QuietStdout()
+    {
+        fflush(stdout);
+        if (saved >= 0) { dup2(saved, 1); close(saved); }
+    }
+};
+
+struct FtzDaz {
+    unsigned int saved[1024];
+    int n;
+    explicit FtzDaz(int threads) : n(threads < 1024 ? threads : 1024)
+    {
+        saved[0] = _mm_getcsr();
+#pragma omp parallel num_threads(n)
+        {
+            int t = omp_get_thread_num();
+            if (t < 1024) saved[t] = _mm_getcsr();
+            _mm_setcsr(_mm_getcsr() | 0x8040u); // FTZ (bit 15) | DAZ (bit 6)
+        }
+        _mm_setcsr(_mm_getcsr() | 0x8040u);
+    }
+    ~FtzDaz()
+    {
+#pragma omp parallel num_threads(n)
+        {
+            int t = omp_get_thread_num();
+            if (t < 1024) _mm_setcsr(saved[t]);
+        }
+    }
+};
+
+// V3/matrix_max_plus_section.c:165-209 dispatches the row remainder mr = min(MR, N_tile-ii)
+// to a register tile of the same NR and calls exit(-1) when none exists. NR=8 and NR=24 have
+// tiles for mr=1..3; NR=16 only for mr=3,4, so every row block must be full.
+bool mrnr_dispatched(long MR, long NR, long N_tile, long R)
+{
+    if ((NR == 8 || NR == 24) && MR >= 1 && MR <= 3) return true;
+    if (NR == 16 && (MR == 3 || MR == 4)) return N_tile % MR == 0 && (N_tile - R) % MR == 0;
+    return false;
+}
+
+} // namespace
+
+extern "C" {
+
+void ref_set_weights(const float *w12);
+
+// Fills the caller's reference-layout buffer F_lin
+// (M*M*N_sec*N_sec*(N_tile+1)*N_tile floats). Returns 0, or -1 for parameters the reference
+// rejects with exit(-1) (V3/bpmax.c:131) or that would overrun its register tiles.
+int ref_bpmax_fill(long M, long N, long N_tile, long MR, long NR, int threads, const int *seq1,
+                   const int *seq2, const float *w12, float *F_lin, int zero_scratch)
+{
+    if (M < 1 || N < 8 || N_tile < 4 || MR < 1 || NR < 1 || threads < 1 || threads > 128) return -1;
+    long N_sec = (N + N_tile - 1) / N_tile;
+    long R = (N_tile - N % N_tile) % N_tile;
+    if (N_sec < 2 || !mrnr_dispatched(MR, NR, N_tile, R) || N_tile % NR != 0 || N_tile < NR) return -1;
+    if (w12) ref_set_weights(w12);
+    const long T = N_tile;
+    float ******F = (float ******)malloc(sizeof(float *****) * M);
+    if (!F) return -1;
+    for (long a = 0; a < M; ++a) {
+        F[a] = (float *****)malloc(sizeof(float ****) * M);
+        for (long b = 0; b < M; ++b) {
+            F[a][b] = (float ****)malloc(sizeof(float ***) * N_sec);
+            for (long c = 0; c < N_sec; ++c) {
+                F[a][b][c] = (float ***)malloc(sizeof(float **) * N_sec);
+                for (long d = 0; d < N_sec; ++d) {
+                    F[a][b][c][d] = (float **)malloc(sizeof(float *) * (T + 1));
+                    for (long e = 0; e <= T; ++e)
+                        F[a][b][c][d][e] = F_lin + ((((a * M + b) * N_sec + c) * N_sec + d) * (T + 1) + e) * T;
+                }
+            }
+        }
+    }
+    int *s1 = (int *)malloc(sizeof(int) * M);
+    int *s2 = (int *)malloc(sizeof(int) * N);
+    memcpy(s1, seq1, sizeof(int) * M);
+    memcpy(s2, seq2, sizeof(int) * N);
+    omp_set_num_threads(threads);
+    if (zero_scratch) mallopt(M_PERTURB, 0xff);
+    {
+        QuietStdout quiet;
+        FtzDaz ftz(threads);
+        bpmax(M, N, N_sec, N_tile, R, MR, NR, threads, s1, s2, F);
+    }
+    if (zero_scratch) mallopt(M_PERTURB, 0);
+    free(s1);
+    free(s2);
+    for (long a = 0; a < M; ++a) {
+        for (long b = 0; b < M; ++b) {
+            for (long c = 0; c < N_sec; ++c) {
+                for (long d = 0; d < N_sec; ++d) free(F[a][b][c][d]);
+                free(F[a][b][c]);
+            }
+            free(F[a][b]);
+        }
+        free(F[a]);
+    }
+    free(F);
+    return 0;
+}
+
+// Runs the reference's memoised verify program into F4 (M*M*N*N floats, [i1][j1][i2][j2],
+// only i1<=j1, i2<=j2 written). Memory ~30*M^2*N^2 bytes: small sizes only.
+int ref_bpmax_verify(long M, long N, const int *seq1, const int *seq2, const float *w12, float *F4)
+{
+    if (M < 1 || N < 8) return -1;
+    if (w12) ref_set_weights(w12);
+    float ****F = (float ****)malloc(sizeof(float ***) * M);
+    for (long a = 0; a < M; ++a) {
+        F[a] = (float ***)malloc(sizeof(float **) * M);
+        for (long b = 0; b < M; ++b) {
+            F[a][b] = (float **)malloc(sizeof(float *) * N);
+            for (long c = 0; c < N; ++c) F[a][b][c] = F4 + ((a * M + b) * N + c) * N;
+        }
+    }
+    int *s1 = (int *)malloc(sizeof(int) * M);
+    int *s2 = (int *)malloc(sizeof(int) * N);
+    memcpy(s1, seq1, sizeof(int) * M);
+    memcpy(s2, seq2, sizeof(int) * N);
+    {
+        QuietStdout quiet;
+        FtzDaz ftz(1);
+        bpmax_verify(M, N, s1, s2, F);
+    }
+    free(s1);
+    free(s2);
+    for (long a = 0; a < M; ++a) {
+        for (long b = 0; b < M; ++b) free(F[a][b]);
+        free(F[a]);
+    }
+    free(F);
+    return 0;
+}
+
+} // extern "C"
