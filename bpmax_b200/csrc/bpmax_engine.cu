@@ -1,0 +1,671 @@
+// bpmax_engine.cu -- host side of the B200 BPMax fill: device arenas, the outer-diagonal
+// schedule, CUDA-graph capture, and the C ABI declared in include/bpmax_gpu.h.
+//
+// Schedule of one fill (any number of pairs of uneven lengths, batched on one stream):
+//   clear F; single-strand tables S1, S2 of every pair;
+//   for d = 0 .. max(M)-1:                     (outer wavefront over j1-i1, V3/bpmax.c:300-323)
+//     R0+R3+R4 product kernel over the cells (i1, i1+d) of every pair with M > d, k1 split
+//       into chunks so that every diagonal launches enough CTAs to fill the GPU;
+//     finalize kernel over the same cells (init, SW1, inner R1/R2/SW2 wavefront, FT copy).
+// The whole sequence is captured once per shape as a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/bpmax_gpu.h"
+#include "bpmax_kernels.cuh"
+
+using namespace bpmax;
+
+namespace {
+
+constexpr int MAX_SMALL_NP = 64;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Plan {
+    std::vector<int> Ms, Ns;
+    std::vector<PairDesc> pairs;
+    long long F_floats = 0, S_floats = 0;
+    int bases_bytes = 0;
+    int maxM = 0;
+    // per diagonal and Np class (index NB-1): ranges in the job arrays
+    struct Launch { int d, nb, first, count; };
+    std::vector<Launch> r0_launches, fin_launches;
+    std::vector<R0Job> r0_jobs;
+    std::vector<CellJob> cell_jobs;
+    cudaGraphExec_t graph = nullptr;
+    long launches = 0;
+};
+
+}  // namespace
+
+struct bpmax_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    Weights W;
+    std::string err;
+    DevBuf F, FT, S, bases, pairs, r0jobs, celljobs, scores, conv;
+    float *host_stage[2] = {nullptr, nullptr};
+    size_t host_stage_bytes = 0;
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    Plan plan;
+    bool plan_valid = false;
+    float last_ms = 0.f;
+    long last_launches = 0;
+};
+
+namespace {
+
+int fail(bpmax_ctx *ctx, int status, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    return status;
+}
+
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? BPMAX_ENOMEM : BPMAX_ECUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
+    } while (0)
+
+int ensure(bpmax_ctx *ctx, DevBuf &b, size_t bytes)
+{
+    if (b.bytes >= bytes) return BPMAX_OK;
+    if (b.p) CK(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = std::max(bytes, (size_t)256);
+    CK(cudaMalloc(&b.p, want));
+    b.bytes = want;
+    return BPMAX_OK;
+}
+
+int weights_ok(const float *w)
+{
+    for (int t = 0; t < 12; ++t)
+        if (!std::isfinite(w[t]) || w[t] < 0.0f || std::signbit(w[t])) return 0;
+    return 1;
+}
+
+long long align64(long long x) { return (x + 63) / 64 * 64; }
+
+// Builds the device layout and the per-diagonal job lists for the given pair shapes.
+int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &Ns, Plan &P)
+{
+    P = Plan();
+    P.Ms = Ms;
+    P.Ns = Ns;
+    const int n = (int)Ms.size();
+    long long f = 0, s = 0;
+    int b = 0;
+    for (int p = 0; p < n; ++p) {
+        PairDesc pd{};
+        pd.M = Ms[p];
+        pd.N = Ns[p];
+        pd.Np = std::max(8, (Ns[p] + 7) / 8 * 8);
+        if (pd.Np > MAX_SMALL_NP)
+            return fail(ctx, BPMAX_EINVAL, "strand-2 length %d > %d is not supported by this build", Ns[p], MAX_SMALL_NP);
+        pd.F_off = f;
+        f = align64(f + (long long)Ms[p] * (Ms[p] + 1) / 2 * pd.Np * pd.Np);
+        pd.S1_off = s;
+        s = align64(s + (long long)Ms[p] * Ms[p]);
+        pd.S2_off = s;
+        s = align64(s + (long long)pd.Np * pd.Np);
+        pd.seq1_off = b;
+        b += Ms[p];
+        pd.seq2_off = b;
+        b += Ns[p];
+        P.pairs.push_back(pd);
+        P.maxM = std::max(P.maxM, Ms[p]);
+    }
+    P.F_floats = f;
+    P.S_floats = s;
+    P.bases_bytes = b;
+    // jobs, grouped by diagonal then Np class
+    const int target = 4 * ctx->sms;  // CTAs per diagonal launch worth splitting k1 for
+    for (int d = 0; d < P.maxM; ++d) {
+        for (int nb = 1; nb <= MAX_SMALL_NP / 8; ++nb) {
+            long long cells = 0;
+            for (int p = 0; p < n; ++p)
+                if (P.pairs[p].Np == 8 * nb && Ms[p] > d) cells += Ms[p] - d;
+            if (cells == 0) continue;
+            Plan::Launch fl{d, nb, (int)P.cell_jobs.size(), 0};
+            for (int p = 0; p < n; ++p)
+                if (P.pairs[p].Np == 8 * nb && Ms[p] > d)
+                    for (int i1 = 0; i1 < Ms[p] - d; ++i1) P.cell_jobs.push_back(CellJob{p, i1});
+            fl.count = (int)P.cell_jobs.size() - fl.first;
+            P.fin_launches.push_back(fl);
+            if (d == 0) continue;
+            long long chunks = std::max(1LL, std::min((long long)d, (target + cells - 1) / cells));
+            int csize = (int)((d + chunks - 1) / chunks);
+            Plan::Launch rl{d, nb, (int)P.r0_jobs.size(), 0};
+            for (int p = 0; p < n; ++p)
+                if (P.pairs[p].Np == 8 * nb && Ms[p] > d)
+                    for (int i1 = 0; i1 < Ms[p] - d; ++i1)
+                        for (int k = i1; k < i1 + d; k += csize)
+                            P.r0_jobs.push_back(R0Job{p, i1, k, std::min(k + csize, i1 + d)});
+            rl.count = (int)P.r0_jobs.size() - rl.first;
+            P.r0_launches.push_back(rl);
+        }
+    }
+    return BPMAX_OK;
+}
+
+template <int NB>
+void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L)
+{
+    using Sh = R0Shape<NB>;
+    r0_small_kernel<NB><<<L.count, Sh::THREADS, Sh::SMEM, ctx->stream>>>(
+        (const R0Job *)ctx->r0jobs.p + L.first, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
+        (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
+}
+
+template <int NB>
+void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L)
+{
+    finalize_small_kernel<8 * NB><<<L.count, 256, 0, ctx->stream>>>(
+        (const CellJob *)ctx->celljobs.p + L.first, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
+        (float *)ctx->FT.p, (const float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W, L.d);
+}
+
+template <int NB>
+int set_smem_attr(bpmax_ctx *ctx)
+{
+    CK(cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<NB>::SMEM));
+    return BPMAX_OK;
+}
+
+struct KernelProfile {
+    bool on = false;
+    cudaEvent_t a = nullptr, b = nullptr;
+    float ms[3] = {0, 0, 0};
+    long launches[3] = {0, 0, 0};
+};
+
+// brackets one launch with events when profiling (eager runs only, never inside a capture)
+struct ProfScope {
+    bpmax_ctx *ctx;
+    KernelProfile *kp;
+    int kind;
+    ProfScope(bpmax_ctx *c, KernelProfile *k, int kind_) : ctx(c), kp(k), kind(kind_)
+    {
+        if (kp && kp->on) cudaEventRecord(kp->a, ctx->stream);
+    }
+    ~ProfScope()
+    {
+        if (kp && kp->on) {
+            cudaEventRecord(kp->b, ctx->stream);
+            cudaEventSynchronize(kp->b);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, kp->a, kp->b);
+            kp->ms[kind] += t;
+            kp->launches[kind] += 1;
+        }
+    }
+};
+
+int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
+{
+    long launches = 0;
+    CK(cudaMemsetAsync(ctx->F.p, 0, (size_t)P.F_floats * sizeof(float), ctx->stream));
+    {
+        ProfScope ps(ctx, kp, 0);
+        single_strand_kernel<<<2 * (int)P.pairs.size(), 512, 0, ctx->stream>>>(
+            (const PairDesc *)ctx->pairs.p, (const uint8_t *)ctx->bases.p, (float *)ctx->S.p, ctx->W);
+    }
+    ++launches;
+    size_t ri = 0, fi = 0;
+    for (int d = 0; d < P.maxM; ++d) {
+        for (; ri < P.r0_launches.size() && P.r0_launches[ri].d == d; ++ri, ++launches) {
+            const auto &L = P.r0_launches[ri];
+            ProfScope ps(ctx, kp, 1);
+            switch (L.nb) {
+            case 1: launch_r0<1>(ctx, L); break;
+            case 2: launch_r0<2>(ctx, L); break;
+            case 3: launch_r0<3>(ctx, L); break;
+            case 4: launch_r0<4>(ctx, L); break;
+            case 5: launch_r0<5>(ctx, L); break;
+            case 6: launch_r0<6>(ctx, L); break;
+            case 7: launch_r0<7>(ctx, L); break;
+            default: launch_r0<8>(ctx, L); break;
+            }
+        }
+        for (; fi < P.fin_launches.size() && P.fin_launches[fi].d == d; ++fi, ++launches) {
+            const auto &L = P.fin_launches[fi];
+            ProfScope ps(ctx, kp, 2);
+            switch (L.nb) {
+            case 1: launch_fin<1>(ctx, L); break;
+            case 2: launch_fin<2>(ctx, L); break;
+            case 3: launch_fin<3>(ctx, L); break;
+            case 4: launch_fin<4>(ctx, L); break;
+            case 5: launch_fin<5>(ctx, L); break;
+            case 6: launch_fin<6>(ctx, L); break;
+            case 7: launch_fin<7>(ctx, L); break;
+            default: launch_fin<8>(ctx, L); break;
+            }
+        }
+    }
+    CK(cudaGetLastError());
+    P.launches = launches;
+    return BPMAX_OK;
+}
+
+// Makes the plan for these shapes current (reusing the cached one and its graph when the
+// shapes repeat) and uploads the sequences. Sequences are validated by the caller.
+int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &Ns,
+            const std::vector<const int *> &s1s, const std::vector<const int *> &s2s)
+{
+    int st;
+    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns)) {
+        if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
+        ctx->plan.graph = nullptr;
+        ctx->plan_valid = false;
+        if ((st = build_plan(ctx, Ms, Ns, ctx->plan)) != BPMAX_OK) return st;
+        Plan &P = ctx->plan;
+        if ((st = ensure(ctx, ctx->F, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->FT, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->S, P.S_floats * sizeof(float))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->bases, P.bases_bytes + 16)) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->pairs, P.pairs.size() * sizeof(PairDesc))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->r0jobs, P.r0_jobs.size() * sizeof(R0Job))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->celljobs, P.cell_jobs.size() * sizeof(CellJob))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->scores, P.pairs.size() * sizeof(float))) != BPMAX_OK) return st;
+        CK(cudaMemcpyAsync(ctx->pairs.p, P.pairs.data(), P.pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, ctx->stream));
+        if (!P.r0_jobs.empty())
+            CK(cudaMemcpyAsync(ctx->r0jobs.p, P.r0_jobs.data(), P.r0_jobs.size() * sizeof(R0Job), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->celljobs.p, P.cell_jobs.data(), P.cell_jobs.size() * sizeof(CellJob), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->plan_valid = true;
+    }
+    // sequences: seq1 as is, seq2 reversed (V3/transform_reverse_1D_to_2D.c:131-135)
+    Plan &P = ctx->plan;
+    std::vector<uint8_t> hb(P.bases_bytes);
+    for (size_t p = 0; p < P.pairs.size(); ++p) {
+        const PairDesc &pd = P.pairs[p];
+        for (int i = 0; i < pd.M; ++i) hb[pd.seq1_off + i] = (uint8_t)s1s[p][i];
+        for (int i = 0; i < pd.N; ++i) hb[pd.seq2_off + i] = (uint8_t)s2s[p][pd.N - 1 - i];
+    }
+    CK(cudaMemcpyAsync(ctx->bases.p, hb.data(), hb.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BPMAX_OK;
+}
+
+// Runs the fill of the current plan (graph captured on first use) and times it.
+int run_fill(bpmax_ctx *ctx)
+{
+    Plan &P = ctx->plan;
+    int st;
+    if (!P.graph) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_fill(ctx, P);
+        cudaGraph_t captured = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(ctx->stream, &captured);
+        if (st != BPMAX_OK) {
+            if (captured) cudaGraphDestroy(captured);
+            return st;
+        }
+        if (ce != cudaSuccess) return fail(ctx, BPMAX_ECUDA, "graph capture: %s", cudaGetErrorString(ce));
+        g = captured;
+        CK(cudaGraphInstantiate(&P.graph, g, 0));
+        cudaGraphDestroy(g);
+    }
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    CK(cudaGraphLaunch(P.graph, ctx->stream));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    gather_scores_kernel<<<((int)P.pairs.size() + 127) / 128, 128, 0, ctx->stream>>>(
+        (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)P.pairs.size(), (float *)ctx->scores.p);
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    ctx->last_launches = P.launches;
+    return BPMAX_OK;
+}
+
+int check_pair(bpmax_ctx *ctx, const int *s1, long M, const int *s2, long N)
+{
+    if (!s1 || !s2) return fail(ctx, BPMAX_EINVAL, "null sequence pointer");
+    if (M < 1 || N < 1) return fail(ctx, BPMAX_EINVAL, "sequence lengths must be >= 1 (M=%ld, N=%ld)", M, N);
+    if (M > 65535 || N > 65535) return fail(ctx, BPMAX_EINVAL, "sequence length too large");
+    for (long i = 0; i < M; ++i)
+        if (s1[i] < 0 || s1[i] > 4) return fail(ctx, BPMAX_EINVAL, "seq1[%ld]=%d is not a base code 0..4", i, s1[i]);
+    for (long i = 0; i < N; ++i)
+        if (s2[i] < 0 || s2[i] > 4) return fail(ctx, BPMAX_EINVAL, "seq2[%ld]=%d is not a base code 0..4", i, s2[i]);
+    return BPMAX_OK;
+}
+
+int fill_pairs(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms, const int *const *seq2s,
+               const long *Ns)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (num_pairs < 1 || !seq1s || !seq2s || !Ms || !Ns) return fail(ctx, BPMAX_EINVAL, "empty batch");
+    std::vector<int> vm(num_pairs), vn(num_pairs);
+    std::vector<const int *> a(num_pairs), b(num_pairs);
+    for (int p = 0; p < num_pairs; ++p) {
+        int st = check_pair(ctx, seq1s[p], Ms[p], seq2s[p], Ns[p]);
+        if (st) return st;
+        vm[p] = (int)Ms[p];
+        vn[p] = (int)Ns[p];
+        a[p] = seq1s[p];
+        b[p] = seq2s[p];
+    }
+    CK(cudaSetDevice(ctx->device));
+    int st = prepare(ctx, vm, vn, a, b);
+    if (st) return st;
+    return run_fill(ctx);
+}
+
+int ensure_host_stage(bpmax_ctx *ctx, size_t bytes)
+{
+    if (ctx->host_stage_bytes >= bytes) return BPMAX_OK;
+    for (int i = 0; i < 2; ++i) {
+        if (ctx->host_stage[i]) cudaFreeHost(ctx->host_stage[i]);
+        ctx->host_stage[i] = nullptr;
+    }
+    ctx->host_stage_bytes = 0;
+    for (int i = 0; i < 2; ++i) CK(cudaMallocHost(&ctx->host_stage[i], bytes));
+    ctx->host_stage_bytes = bytes;
+    return BPMAX_OK;
+}
+
+bool is_pinned(const void *p)
+{
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bpmax_gpu_status_string(int s)
+{
+    switch (s) {
+    case BPMAX_OK: return "ok";
+    case BPMAX_EINVAL: return "invalid argument";
+    case BPMAX_ENOMEM: return "out of memory";
+    case BPMAX_ECUDA: return "CUDA error";
+    case BPMAX_ENODEV: return "no usable CUDA device";
+    case BPMAX_ETIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int bpmax_gpu_create(int device, bpmax_ctx **out)
+{
+    if (!out) return BPMAX_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return BPMAX_ENODEV;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        return BPMAX_ENODEV;  // the kernels are built for sm_100a only
+    }
+    bpmax_ctx *ctx = new bpmax_ctx();
+    ctx->device = device;
+    ctx->sms = prop.multiProcessorCount;
+    const float ref_w[12] = {1.0f, 1.0f, 3.0f, 3.0f, 1.5f, 1.5f, 1.0f, 1.0f, 3.0f, 3.0f, 1.5f, 1.5f};
+    memcpy(ctx->W.w, ref_w, sizeof ref_w);
+    int st = BPMAX_OK;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->stage_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->stage_ev[1], cudaEventDisableTiming) != cudaSuccess)
+        st = BPMAX_ECUDA;
+    if (st == BPMAX_OK) st = set_smem_attr<1>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<2>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<3>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<4>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<5>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<6>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<7>(ctx);
+    if (st == BPMAX_OK) st = set_smem_attr<8>(ctx);
+    if (st != BPMAX_OK) {
+        cudaGetLastError();
+        bpmax_gpu_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return BPMAX_OK;
+}
+
+void bpmax_gpu_destroy(bpmax_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
+    for (DevBuf *b : {&ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs, &ctx->r0jobs, &ctx->celljobs,
+                      &ctx->scores, &ctx->conv})
+        if (b->p) cudaFree(b->p);
+    for (int i = 0; i < 2; ++i) {
+        if (ctx->host_stage[i]) cudaFreeHost(ctx->host_stage[i]);
+        if (ctx->stage_ev[i]) cudaEventDestroy(ctx->stage_ev[i]);
+    }
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *bpmax_gpu_last_error(const bpmax_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int bpmax_gpu_set_weights(bpmax_ctx *ctx, const float *w)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (!w || !weights_ok(w)) return fail(ctx, BPMAX_EINVAL, "weights must be 12 finite values >= +0");
+    memcpy(ctx->W.w, w, sizeof ctx->W.w);
+    // weights are kernel arguments baked into the captured graph: recapture on next use
+    if (ctx->plan.graph) {
+        cudaGraphExecDestroy(ctx->plan.graph);
+        ctx->plan.graph = nullptr;
+    }
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_score(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *score)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    int st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N);
+    if (st) return st;
+    if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_score_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                          const int *const *seq2s, const long *Ns, float *scores)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    int st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
+    if (st) return st;
+    if (scores) CK(cudaMemcpy(scores, ctx->scores.p, num_pairs * sizeof(float), cudaMemcpyDeviceToHost));
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_score_each(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                         const int *const *seq2s, const long *Ns, float *scores)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (num_pairs < 1) return fail(ctx, BPMAX_EINVAL, "empty batch");
+    float total = 0.f;
+    long launches = 0;
+    for (int p = 0; p < num_pairs; ++p) {
+        int st = fill_pairs(ctx, 1, seq1s + p, Ms + p, seq2s + p, Ns + p);
+        if (st) return st;
+        total += ctx->last_ms;
+        launches += ctx->last_launches;
+        if (scores) CK(cudaMemcpy(scores + p, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+    }
+    ctx->last_ms = total;
+    ctx->last_launches = launches;
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_fill_compact(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *F_compact,
+                           float *score)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    int st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N);
+    if (st) return st;
+    if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+    if (!F_compact) return BPMAX_OK;
+    const PairDesc &pd = ctx->plan.pairs[0];
+    const long long n_out = M * (M + 1) / 2 * N * N;
+    if ((st = ensure(ctx, ctx->conv, n_out * sizeof(float))) != BPMAX_OK) return st;
+    to_compact_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>((const float *)ctx->F.p + pd.F_off, (int)M, (int)N,
+                                                             pd.Np, n_out, (float *)ctx->conv.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(F_compact, ctx->conv.p, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, long N_tile, float *F_lin,
+                   float *score)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    // preconditions of V3/bpmax.c:131 (N_sec>=2 and 0<=R<N_tile follow from the layout)
+    if (M < 1 || N < 8 || N_tile < 4) return fail(ctx, BPMAX_EINVAL, "The value of parameters are not valid.");
+    const long Ns = (N + N_tile - 1) / N_tile;
+    if (Ns < 2) return fail(ctx, BPMAX_EINVAL, "The value of parameters are not valid. (N_sec=%ld < 2)", Ns);
+    int st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N);
+    if (st) return st;
+    if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+    if (!F_lin) return BPMAX_OK;
+    const PairDesc &pd = ctx->plan.pairs[0];
+    const long long cell_f = (long long)Ns * Ns * (N_tile + 1) * N_tile;
+    // outer row i1 of the reference layout: cells (i1, i1..M-1) are contiguous
+    const long long row_max = (long long)M * cell_f;
+    if ((st = ensure(ctx, ctx->conv, 2 * row_max * sizeof(float))) != BPMAX_OK) return st;
+    const bool pinned = is_pinned(F_lin);
+    if (!pinned && (st = ensure_host_stage(ctx, row_max * sizeof(float))) != BPMAX_OK) return st;
+    std::vector<long long> pending_n(2, 0);
+    std::vector<float *> pending_dst(2, nullptr);
+    for (long i1 = 0; i1 < M; ++i1) {
+        const int slot = (int)(i1 & 1);
+        float *dbuf = (float *)ctx->conv.p + slot * row_max;
+        const long long n_out = (M - i1) * cell_f;
+        float *dst = F_lin + (i1 * M + i1) * cell_f;
+        if (!pinned && pending_dst[slot]) {  // drain the staging buffer this slot used before
+            CK(cudaEventSynchronize(ctx->stage_ev[slot]));
+            memcpy(pending_dst[slot], ctx->host_stage[slot], pending_n[slot] * sizeof(float));
+            pending_dst[slot] = nullptr;
+        }
+        to_reference_row_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>(
+            (const float *)ctx->F.p + pd.F_off, (int)M, (int)N, pd.Np, (int)N_tile, (int)Ns, (int)i1, n_out, dbuf);
+        CK(cudaGetLastError());
+        if (pinned) {
+            CK(cudaMemcpyAsync(dst, dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        } else {
+            CK(cudaMemcpyAsync(ctx->host_stage[slot], dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaEventRecord(ctx->stage_ev[slot], ctx->stream));
+            pending_dst[slot] = dst;
+            pending_n[slot] = n_out;
+        }
+    }
+    for (int slot = 0; slot < 2; ++slot)
+        if (!pinned && pending_dst[slot]) {
+            CK(cudaEventSynchronize(ctx->stage_ev[slot]));
+            memcpy(pending_dst[slot], ctx->host_stage[slot], pending_n[slot] * sizeof(float));
+        }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int, const int *const *, const long *, const int *const *, const long *,
+                         float *, float *)
+{
+    return fail(ctx, BPMAX_EINVAL, "gradients are not available in this build");
+}
+
+int bpmax_gpu_profile_kernels(bpmax_ctx *ctx, float *ms, long *launches, double *terms)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (!ctx->plan_valid) return fail(ctx, BPMAX_EINVAL, "no fill has run on this context");
+    CK(cudaSetDevice(ctx->device));
+    KernelProfile kp;
+    kp.on = true;
+    CK(cudaEventCreate(&kp.a));
+    CK(cudaEventCreate(&kp.b));
+    int st = enqueue_fill(ctx, ctx->plan, &kp);
+    cudaEventDestroy(kp.a);
+    cudaEventDestroy(kp.b);
+    if (st) return st;
+    CK(cudaStreamSynchronize(ctx->stream));
+    // algorithmic candidates per kind
+    auto C = [](double n) { return n * (n * n - 1) / 6.0; };
+    auto T = [](double n) { return n * (n + 1) / 2.0; };
+    double t[3] = {0, 0, 0};
+    for (const PairDesc &pd : ctx->plan.pairs) {
+        t[0] += C(pd.M) + C(pd.N);
+        t[1] += C(pd.M) * (C(pd.N) + 2 * T(pd.N));
+        t[2] += 2 * T(pd.M) * C(pd.N);
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (ms) ms[k] = kp.ms[k];
+        if (launches) launches[k] = kp.launches[k];
+        if (terms) terms[k] = t[k];
+    }
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s)
+{
+    if (!ctx || !terms_per_s) return BPMAX_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    float *buf = nullptr;
+    const int grid = ctx->sms * 8, block = 128, reps = 4000;
+    CK(cudaMalloc(&buf, (size_t)grid * block * sizeof(float) + 64 * sizeof(float)));
+    std::vector<float> h(64);
+    for (int i = 0; i < 64; ++i) h[i] = (float)(i % 17);
+    cudaMemcpyAsync(buf, h.data(), 64 * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    maxplus_peak_kernel<<<grid, block, 0, ctx->stream>>>(buf, buf + 64, reps);
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    for (int i = 0; i < 3; ++i) maxplus_peak_kernel<<<grid, block, 0, ctx->stream>>>(buf, buf + 64, reps);
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    cudaError_t e = cudaEventSynchronize(ctx->ev1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(ctx, BPMAX_ECUDA, "peak probe: %s", cudaGetErrorString(e));
+    *terms_per_s = 3.0 * grid * block * (double)reps * 128.0 / (ms * 1e-3);
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (fill_ms) *fill_ms = ctx->last_ms;
+    if (launches) *launches = ctx->last_launches;
+    return BPMAX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+/*
+ * bpmax_gpu.h -- C ABI of the B200 (sm_100a) BPMax fill engine, libbpmax_gpu.so.
+ *
+ * Plain pointers and sizes only. Every entry point returns a bpmax_status; on failure
+ * bpmax_gpu_last_error() gives a message. A context owns one CUDA device, one stream and its
+ * device buffers; use one context per host thread.
+ *
+ * Reference interface replaced (paths relative to the reference project root, with
+ * V3 = TPDS/source/release/MPT_RT_V3/bpmax_complete_otf_ftable/src):
+ *   void bpmax(long M, long N, long N_sec, long N_tile, long R, long MR, long NR, long P,
+ *              int* seq1, int* seq2, float****** FTable)                     V3/bpmax.c:129
+ * The C++ symbol itself is exported by libbpmax_gpu.so too (bpmax_b200/csrc/bpmax_shim.cpp),
+ * so the reference's CLI wrapper V3/bpmax-wrapper.c links against this library unchanged.
+ *
+ * Sequences are int arrays of bases 0..3 = A,C,G,U (4 = any other letter), the encoding of
+ * toNum in V3/external_functions.c:70-85. Strand 2 is consumed reversed, as in the reference.
+ * Weights are a 12-entry table: intra-strand AU,UA,GC,CG,GU,UG then inter-strand
+ * AU,UA,GC,CG,GU,UG; every weight must be finite and >= +0. The reference's hard-coded values
+ * (V3/external_functions.c:58-68) are AU=UA=1.0, GC=CG=3, GU=UG=1.5 on both strands.
+ */
+#ifndef BPMAX_GPU_H
+#define BPMAX_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bpmax_status {
+    BPMAX_OK = 0,
+    BPMAX_EINVAL = 1,   /* invalid argument (the reference prints and calls exit(-1)) */
+    BPMAX_ENOMEM = 2,   /* device or pinned host allocation failed */
+    BPMAX_ECUDA = 3,    /* a CUDA call failed */
+    BPMAX_ENODEV = 4,   /* no CUDA device, or the kernels were not built for it */
+    BPMAX_ETIMEOUT = 5  /* a device-side bounded wait gave up; the context stays usable */
+} bpmax_status;
+
+typedef struct bpmax_ctx bpmax_ctx;
+
+/* Context life cycle. device = CUDA ordinal. */
+int bpmax_gpu_create(int device, bpmax_ctx **out);
+void bpmax_gpu_destroy(bpmax_ctx *ctx);
+const char *bpmax_gpu_last_error(const bpmax_ctx *ctx);
+const char *bpmax_gpu_status_string(int status);
+
+/* Score weights used by later calls (default: the reference's values).
+ * Replaces the link-time hook e_intra_score/e_inter_score, V3/external_functions.c:58-68. */
+int bpmax_gpu_set_weights(bpmax_ctx *ctx, const float *weights12);
+
+/* Fill of one pair into the reference's linear F layout, host memory:
+ * F_lin = &FTable[0][0][0][0][0][0] of a float[M][M][N_sec][N_sec][N_tile+1][N_tile] buffer,
+ * N_sec = ceil(N/N_tile), R = (N_tile - N % N_tile) % N_tile, logical cell
+ * (i1,j1,i2,j2) at [i1][j1][(i2+R)/N_tile][(j2+R)/N_tile][(i2+R)%N_tile][(j2+R)%N_tile]
+ * (V3/bpmax-wrapper.c:44, :175-197). Writes exactly the cells the reference fill writes
+ * (logical cells, -FLT_MAX below the diagonal of diagonal tiles and in their halo row, and the
+ * halo row of off-diagonal tiles = row 0 of the tile below). Cells the reference leaves
+ * unwritten inside outer cells i1<=j1 (tiles with I2>J2, padding rows and columns) receive NaN;
+ * outer cells i1>j1 are not touched. F_lin may be pinned (cudaHostAlloc) for direct copies.
+ * score (may be NULL) receives F(0,M-1,0,N-1). Preconditions as the reference
+ * (V3/bpmax.c:131): M>=1, N>=8, N_tile>=4, N_sec>=2, 0<=R<N_tile.
+ * Replaces V3/bpmax.c:129 (the tiling arguments MR, NR, P only tune the CPU code). */
+int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, long N_tile,
+                   float *F_lin, float *score);
+
+/* Fill of one pair into the compact layout, host memory: T(M)=M(M+1)/2 outer cells in
+ * row-major upper-triangle order, each an N x N inner table [i2][j2]; cells with i2>j2 are
+ * -FLT_MAX. Same logical values as bpmax_gpu_fill. F_compact may be NULL (score only). */
+int bpmax_gpu_fill_compact(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N,
+                           float *F_compact, float *score);
+
+/* Optimal score F(0,M-1,0,N-1) of one pair, the value V3/bpmax-wrapper.c:281 prints. */
+int bpmax_gpu_score(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *score);
+
+/* Scores of many pairs of uneven lengths in one batched fill (no reference counterpart: the
+ * reference fills one pair per process run). seq1s/seq2s: per-pair host pointers; M>=1, N>=1
+ * per pair. scores: num_pairs floats. */
+int bpmax_gpu_score_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                          const int *const *seq2s, const long *Ns, float *scores);
+
+/* Same pairs, one fill launch sequence per pair (the baseline the batched fill is compared to). */
+int bpmax_gpu_score_each(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                         const int *const *seq2s, const long *Ns, float *scores);
+
+/* Forward fill plus adjoint (backward) pass of many pairs: grads[12*p + t] = d score_p / d w_t,
+ * the number of times weight t is used by the optimal structure of pair p, found by following
+ * argmax edges with the reference's tie-break (the later candidate of __max_float(x,y) =
+ * x>y?x:y wins a tie, V3/bpmax_verify.c:576 order; the last k wins inside a reduction). No
+ * reference counterpart: the reference has neither traceback nor weights as parameters. */
+int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                         const int *const *seq2s, const long *Ns, float *scores, float *grads);
+
+/* Device time in milliseconds of the last fill call's kernels (CUDA events on the context's
+ * stream), and the number of kernel launches it issued. */
+int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches);
+
+/* Re-runs the last fill's kernels one launch at a time with CUDA events around each launch on
+ * the context's stream. Per kernel kind k (0 single-strand, 1 R0+R3+R4 product, 2 finalize /
+ * inner wavefront): ms[k] = summed launch durations, launches[k] = launch count, terms[k] =
+ * algorithmic max-plus candidates (one fp32 add + one max each) the kind evaluates. Arrays of 3.
+ * No reference counterpart (measurement only). */
+int bpmax_gpu_profile_kernels(bpmax_ctx *ctx, float *ms, long *launches, double *terms);
+
+/* Measured max-plus issue ceiling of this GPU: a register-resident kernel that runs the
+ * instruction mix of the product kernel's inner loop (fp32 add + 3-input max, no memory traffic)
+ * on every SM. terms_per_s receives candidates per second. No reference counterpart. */
+int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

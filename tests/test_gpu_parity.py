@@ -1,0 +1,130 @@
+"""CUDA fill vs the reference's golden fixtures and the oracle: bit-exact on every cell."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import golden_cases as G
+from bpmax_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from bpmax_b200 import Engine
+
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("case", G.cases(), ids=lambda c: c["name"])
+def test_golden_compact(eng, case):
+    s1, s2, w = G.decode(case["seq1"]), G.decode(case["seq2"]), G.weights(case)
+    eng.set_weights(w)
+    F, score = eng.fill_compact(s1, s2)
+    assert score == case["score"]
+    assert G.sha(F) == case["logical_sha256"]
+    full = G.full_table(case)
+    if full is not None:
+        assert np.array_equal(bits(full), bits(F))
+
+
+@pytest.mark.parametrize("case", [c for c in G.cases() if "reference_layout_sha256" in c], ids=lambda c: c["name"])
+def test_golden_reference_layout(eng, case, oracle_mod):
+    s1, s2, w = G.decode(case["seq1"]), G.decode(case["seq2"]), G.weights(case)
+    M, N, T = case["M"], case["N"], case["N_tile"]
+    eng.set_weights(w)
+    Fr, score = eng.fill(s1, s2, T)
+    mask = oracle_mod.reference_written_mask(M, N, T)
+    assert score == case["score"]
+    assert G.sha(Fr[mask]) == case["reference_layout_sha256"]
+    # outer cells i1 > j1 are never touched (the caller's NaN fill survives)
+    Ns = (N + T - 1) // T
+    V = Fr.reshape(M, M, -1)
+    lower = np.tril(np.ones((M, M), dtype=bool), -1)
+    assert np.isnan(V[lower]).all()
+
+
+@pytest.mark.parametrize("M,N,seed,wkind", [
+    (1, 1, 1, "int"), (1, 5, 2, "int"), (3, 1, 3, "int"), (4, 4, 4, "int"), (2, 9, 5, "real"),
+    (7, 8, 6, "int"), (13, 31, 7, "real"), (22, 33, 8, "int"), (17, 47, 9, "real"), (30, 64, 10, "int"),
+    (9, 57, 11, "real"), (40, 17, 12, "int"), (5, 64, 13, "real"),
+])
+def test_random_vs_oracle(eng, oracle_mod, M, N, seed, wkind):
+    s1, s2 = W.pair(M, N, seed)
+    w = W.INTEGER_WEIGHTS if wkind == "int" else W.random_weights(seed)
+    eng.set_weights(w)
+    F, score = eng.fill_compact(s1, s2)
+    Fo, _, _ = oracle_mod.fill(s1, s2, w)
+    assert np.array_equal(bits(F), bits(Fo))
+    assert score == oracle_mod.score(Fo, M, N)
+
+
+def test_gc_rich_and_reference_weights(eng, oracle_mod):
+    for (M, N, seed, gc, w) in [(26, 40, 21, True, W.INTEGER_WEIGHTS), (19, 24, 22, False, W.REFERENCE_WEIGHTS)]:
+        s1, s2 = W.pair(M, N, seed, W.GC_RICH if gc else None)
+        eng.set_weights(w)
+        F, _ = eng.fill_compact(s1, s2)
+        Fo, _, _ = oracle_mod.fill(s1, s2, w)
+        assert np.array_equal(bits(F), bits(Fo))
+
+
+def test_batched_uneven_matches_oracle_and_each(eng, oracle_mod):
+    wl = W.batched_uneven(num_pairs=24, seed=77, m_range=(1, 40), n_range=(1, 64))
+    eng.set_weights(wl.weights)
+    got = eng.score_batch(wl.pairs)
+    each = eng.score_each(wl.pairs)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, wl.weights)[0], len(a), len(b)) for a, b in wl.pairs],
+                   dtype=np.float32)
+    assert np.array_equal(bits(got), bits(exp))
+    assert np.array_equal(bits(each), bits(exp))
+
+
+def test_repeated_calls_and_shape_changes(eng, oracle_mod):
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    for (M, N, seed) in [(12, 20, 31), (12, 20, 32), (6, 44, 33), (12, 20, 31)]:
+        s1, s2 = W.pair(M, N, seed)
+        assert eng.score(s1, s2) == oracle_mod.score(oracle_mod.fill(s1, s2, W.INTEGER_WEIGHTS)[0], M, N)
+
+
+def test_invalid_arguments_rejected(eng):
+    from bpmax_b200 import BpmaxError
+
+    with pytest.raises(BpmaxError):
+        eng.score([0, 1, 5], [1, 2])
+    with pytest.raises(BpmaxError):
+        eng.set_weights([1.0] * 11 + [-1.0])
+    with pytest.raises(BpmaxError):
+        eng.fill([0, 1, 2], [1, 2, 3, 0, 1], 4)  # N < 8: the reference rejects it (V3/bpmax.c:131)
+    # the context stays usable after an error
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    assert eng.score([0, 1, 2, 3, 0, 2, 1, 3, 3], [3, 2, 1, 0, 2, 2]) >= 0
+
+
+def test_dropin_shim_links_like_reference_wrapper(tmp_path, oracle_mod):
+    """Compiles a caller that allocates F exactly like V3/bpmax-wrapper.c and calls bpmax()."""
+    from bpmax_b200 import api
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = str(tmp_path / "shim_harness")
+    libdir = os.path.dirname(api.LIB_PATH)
+    subprocess.run(["g++", "-O2", "-o", exe, os.path.join(here, "shim_harness.cpp"), f"-L{libdir}", "-lbpmax_gpu",
+                    f"-Wl,-rpath,{libdir}"], check=True)
+    M, N, T = 11, 21, 8
+    s1, s2 = W.pair(M, N, 41)
+    inp = " ".join(map(str, list(s1) + list(s2)))
+    out = str(tmp_path / "F.bin")
+    r = subprocess.run([exe, str(M), str(N), str(T), out], input=inp, capture_output=True, text=True, check=True)
+    Fr = np.fromfile(out, dtype=np.float32)
+    Fo, _, _ = oracle_mod.fill(s1, s2, W.REFERENCE_WEIGHTS)  # the shim uses the reference's weights
+    mask = oracle_mod.reference_written_mask(M, N, T)
+    mine = oracle_mod.to_reference_layout(Fo, M, N, T)
+    assert np.array_equal(bits(mine[mask]), bits(Fr[mask]))
+    assert f"F(0,{M - 1},0,{N - 1})" in r.stdout
