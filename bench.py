@@ -41,11 +41,15 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched pairs/s sub-measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--pair", default=None, help="M,N: one custom uniform pair instead of the workload")
     return ap.parse_args()
 
 
-def workload(name: str, rank: int) -> W.Workload:
+def workload(name: str, rank: int, pair: str | None = None) -> W.Workload:
     seed = 2 + 1000 * rank
+    if pair:
+        m, n = (int(x) for x in pair.split(","))
+        return W.single_pair(m, n, seed=seed)
     if name == "single":
         return W.single_pair(1024, 64, seed=seed)
     if name == "small":
@@ -237,7 +241,7 @@ def main_reference(args, world, rank):
 def main_b200(args, world, rank, local):
     from bpmax_b200 import Engine
 
-    wl = workload(args.workload, rank)
+    wl = workload(args.workload, rank, args.pair)
     eng = Engine(local)
     eng.set_weights(wl.weights)
     single = len(wl.pairs) == 1
@@ -286,7 +290,7 @@ def main_b200(args, world, rank, local):
         e2e = measure_e2e(eng, wl, args, world)
 
     batched = None
-    if not args.no_batched and single and args.workload == "single" and world == 1:
+    if not args.no_batched and single and args.workload == "single" and not args.pair and world == 1:
         batched = measure_batched(eng)
         eng.set_weights(wl.weights)
 
