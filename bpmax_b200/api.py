@@ -64,6 +64,7 @@ def load_library():
     L.bpmax_gpu_last_timing.argtypes = [vp, P(c_float), P(c_long)]
     L.bpmax_gpu_profile_kernels.argtypes = [vp, vp, vp, vp]
     L.bpmax_gpu_maxplus_peak.argtypes = [vp, P(ctypes.c_double)]
+    L.bpmax_gpu_score_noalloc.argtypes = [vp, c_long, vp, c_long, vp, vp, vp]
     for name in header_functions():
         if name not in ("bpmax_gpu_destroy", "bpmax_gpu_last_error", "bpmax_gpu_status_string"):
             getattr(L, name).restype = c_int
@@ -80,6 +81,20 @@ def _seq(s) -> np.ndarray:
 
 def _ptr(a: np.ndarray):
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def score_noalloc(seq1, seq2, w12, stream: int | None = None) -> float:
+    """bpmax_gpu_score_noalloc: one pair's score with no memory allocated by the library (its
+    scratch is a fixed 64 MiB device array). Raises BpmaxError on a non-zero status."""
+    L = load_library()
+    a, b = _seq(seq1), _seq(seq2)
+    w = np.ascontiguousarray(np.asarray(w12, dtype=np.float32))
+    out = np.zeros(1, dtype=np.float32)
+    st = L.bpmax_gpu_score_noalloc(_ptr(a), len(a), _ptr(b), len(b), _ptr(w), _ptr(out),
+                                   ctypes.c_void_p(stream) if stream else None)
+    if st != 0:
+        raise BpmaxError(st, "bpmax_gpu_score_noalloc failed")
+    return float(out[0])
 
 
 class Engine:

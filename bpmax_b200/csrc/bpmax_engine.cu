@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -669,3 +670,193 @@ int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches)
 }
 
 }  // extern "C"
+
+// =========================================================================================
+// Allocation-free score entry point (bpmax_gpu_score_noalloc).
+//
+// Some callers cannot allocate device memory: code that runs inside another framework's
+// memory pool or under a fixed device-memory budget (where a raw cudaMalloc is forbidden or
+// would exceed the budget), and latency-sensitive callers that must not risk the implicit
+// device synchronisation cudaMalloc/cudaFree can cause. For them the fill's scratch (the F and
+// FT tables, S1/S2, the sequences and the job lists) lives in one fixed file-scope device array
+// instead of the context's arenas. Every GPU that loads this library holds that array until
+// the process exits.
+// =========================================================================================
+namespace {
+
+constexpr size_t NOALLOC_FLOATS = (size_t)16 << 20;  // 64 MiB of fp32 scratch
+
+static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_FLOATS];
+
+struct NoallocDevice {
+    float *ptr = nullptr;  // device address of g_noalloc_scratch on this device
+    int sms = 0;
+};
+std::mutex g_noalloc_mu;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+
+// sequences (int32, seq1 then seq2) -> base codes (seq1, then seq2 reversed); cell job list
+__global__ void noalloc_prep_kernel(const int *__restrict__ seqs, int M, int N, uint8_t *__restrict__ bases,
+                                    CellJob *__restrict__ cells)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M + N; i += gridDim.x * blockDim.x) {
+        bases[i] = (uint8_t)(i < M ? seqs[i] : seqs[M + (N - 1 - (i - M))]);
+        if (i < M) cells[i] = CellJob{0, i};
+    }
+}
+
+// R0 jobs of diagonal d: cells (i1, i1+d), k1 chunks of csize
+__global__ void noalloc_r0_jobs_kernel(R0Job *__restrict__ jobs, int cells, int d, int csize, int per_cell)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= cells * per_cell) return;
+    const int i1 = q / per_cell, c = q % per_cell;
+    const int a = i1 + c * csize;
+    jobs[q] = R0Job{0, i1, a, min(a + csize, i1 + d)};
+}
+
+template <int NB>
+int noalloc_set_attr()
+{
+    return cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)R0Shape<NB>::SMEM) == cudaSuccess ? BPMAX_OK : BPMAX_ECUDA;
+}
+
+// Once per device, with that device current: the device address of the scratch array (a host
+// reference to g_noalloc_scratch is only a host-side stand-in) and the kernels' attributes.
+int noalloc_setup(int dev, NoallocDevice *out)
+{
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoallocDevice &nd = g_noalloc_dev[dev];
+    if (!nd.ptr) {
+        float *p = nullptr;
+        if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return BPMAX_ECUDA;
+        }
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return BPMAX_ECUDA;
+        int st = noalloc_set_attr<1>();
+        if (!st) st = noalloc_set_attr<2>();
+        if (!st) st = noalloc_set_attr<3>();
+        if (!st) st = noalloc_set_attr<4>();
+        if (!st) st = noalloc_set_attr<5>();
+        if (!st) st = noalloc_set_attr<6>();
+        if (!st) st = noalloc_set_attr<7>();
+        if (!st) st = noalloc_set_attr<8>();
+        if (st) return st;
+        nd.sms = sms;
+        nd.ptr = p;
+    }
+    *out = nd;
+    return BPMAX_OK;
+}
+
+template <int NB>
+void noalloc_launch_diag(cudaStream_t s, int d, int n_r0, int n_cells, const R0Job *rj, const CellJob *cj,
+                         const PairDesc *pd, float *F, float *FT, float *S, const uint8_t *bases, const Weights &W)
+{
+    if (d > 0)
+        r0_small_kernel<NB><<<n_r0, R0Shape<NB>::THREADS, R0Shape<NB>::SMEM, s>>>(rj, pd, F, FT, S, d);
+    finalize_small_kernel<8 * NB><<<n_cells, 256, 0, s>>>(cj, pd, F, FT, S, bases, W, d);
+}
+
+}  // namespace
+
+extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2, long N, const float *weights12,
+                                       float *score, void *stream)
+{
+    if (!seq1 || !seq2 || !weights12 || !score || M < 1 || N < 1 || M > 65535 || N > MAX_SMALL_NP)
+        return BPMAX_EINVAL;
+    for (long i = 0; i < M; ++i)
+        if (seq1[i] < 0 || seq1[i] > 4) return BPMAX_EINVAL;
+    for (long i = 0; i < N; ++i)
+        if (seq2[i] < 0 || seq2[i] > 4) return BPMAX_EINVAL;
+    if (!weights_ok(weights12)) return BPMAX_EINVAL;
+    const int Np = std::max(8, (int)(N + 7) / 8 * 8);
+    const int nb = Np / 8;
+    // scratch layout (floats), every region 256-byte aligned
+    const long long nF = (long long)M * (M + 1) / 2 * Np * Np;
+    const long long off_FT = align64(nF);
+    const long long off_S = off_FT + align64(nF);
+    const long long S2_rel = align64((long long)M * M);
+    const long long off_seq = off_S + align64(S2_rel + (long long)Np * Np);
+    const long long off_bases = off_seq + align64(M + N);
+    const long long off_pd = off_bases + align64((M + N + 3) / 4);
+    const long long off_score = off_pd + align64((long long)(sizeof(PairDesc) + 3) / 4);
+    const long long off_cj = off_score + 64;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        cudaGetLastError();
+        return BPMAX_ENODEV;
+    }
+    NoallocDevice nd;
+    int st = noalloc_setup(dev, &nd);
+    if (st) return st;
+    const int target = 4 * nd.sms;
+    const long long off_rj = off_cj + align64(2LL * M);
+    const long long total = off_rj + 4LL * (M + target + 1);
+    if ((size_t)total > NOALLOC_FLOATS) return BPMAX_EINVAL;  // pair too large for the fixed scratch
+
+    cudaStream_t s = (cudaStream_t)stream;
+    float *base = nd.ptr;
+    float *F = base, *FT = base + off_FT, *S = base + off_S;
+    int *seqs = reinterpret_cast<int *>(base + off_seq);
+    uint8_t *bases = reinterpret_cast<uint8_t *>(base + off_bases);
+    PairDesc *pdp = reinterpret_cast<PairDesc *>(base + off_pd);
+    float *dscore = base + off_score;
+    CellJob *cj = reinterpret_cast<CellJob *>(base + off_cj);
+    R0Job *rj = reinterpret_cast<R0Job *>(base + off_rj);
+    PairDesc pd{};
+    pd.M = (int)M;
+    pd.N = (int)N;
+    pd.Np = Np;
+    pd.F_off = 0;
+    pd.S1_off = 0;
+    pd.S2_off = S2_rel;
+    pd.seq1_off = 0;
+    pd.seq2_off = (int)M;
+    Weights W;
+    memcpy(W.w, weights12, sizeof W.w);
+
+    auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+    // pageable host sources: the copies are staged before cudaMemcpyAsync returns
+    if (!ok(cudaMemcpyAsync(seqs, seq1, sizeof(int) * M, cudaMemcpyHostToDevice, s)) ||
+        !ok(cudaMemcpyAsync(seqs + M, seq2, sizeof(int) * N, cudaMemcpyHostToDevice, s)) ||
+        !ok(cudaMemcpyAsync(pdp, &pd, sizeof pd, cudaMemcpyHostToDevice, s)) ||
+        !ok(cudaMemsetAsync(F, 0, sizeof(float) * nF, s))) {  // F starts at +0 on every call
+        cudaGetLastError();
+        return BPMAX_ECUDA;
+    }
+    noalloc_prep_kernel<<<8, 256, 0, s>>>(seqs, (int)M, (int)N, bases, cj);
+    single_strand_kernel<<<2, 512, 0, s>>>(pdp, bases, S, W);
+    for (int d = 0; d < (int)M; ++d) {
+        const int cells = (int)M - d;
+        int n_r0 = 0;
+        if (d > 0) {
+            const long long chunks = std::max(1LL, std::min((long long)d, (long long)(target + cells - 1) / cells));
+            const int csize = (int)((d + chunks - 1) / chunks);
+            const int per_cell = (d + csize - 1) / csize;
+            n_r0 = cells * per_cell;
+            noalloc_r0_jobs_kernel<<<(n_r0 + 255) / 256, 256, 0, s>>>(rj, cells, d, csize, per_cell);
+        }
+        switch (nb) {
+        case 1: noalloc_launch_diag<1>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 2: noalloc_launch_diag<2>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 3: noalloc_launch_diag<3>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 4: noalloc_launch_diag<4>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 5: noalloc_launch_diag<5>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 6: noalloc_launch_diag<6>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 7: noalloc_launch_diag<7>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        default: noalloc_launch_diag<8>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        }
+    }
+    gather_scores_kernel<<<1, 32, 0, s>>>(pdp, F, 1, dscore);
+    if (!ok(cudaGetLastError()) || !ok(cudaMemcpyAsync(score, dscore, sizeof(float), cudaMemcpyDeviceToHost, s)) ||
+        !ok(cudaStreamSynchronize(s))) {
+        cudaGetLastError();
+        return BPMAX_ECUDA;
+    }
+    return BPMAX_OK;
+}
