@@ -176,8 +176,9 @@ template <int NB>
 void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L)
 {
     using Sh = R0Shape<NB>;
-    r0_small_kernel<NB><<<L.count, Sh::THREADS, Sh::SMEM, ctx->stream>>>(
-        (const R0Job *)ctx->r0jobs.p + L.first, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
+    const int grid = std::min(L.count, 3 * ctx->sms);  // resident CTAs; each loops over jobs
+    r0_small_kernel<NB><<<grid, Sh::THREADS, Sh::SMEM, ctx->stream>>>(
+        (const R0Job *)ctx->r0jobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
         (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
 }
 
@@ -754,11 +755,12 @@ int noalloc_setup(int dev, NoallocDevice *out)
 }
 
 template <int NB>
-void noalloc_launch_diag(cudaStream_t s, int d, int n_r0, int n_cells, const R0Job *rj, const CellJob *cj,
+void noalloc_launch_diag(cudaStream_t s, int sms, int d, int n_r0, int n_cells, const R0Job *rj, const CellJob *cj,
                          const PairDesc *pd, float *F, float *FT, float *S, const uint8_t *bases, const Weights &W)
 {
     if (d > 0)
-        r0_small_kernel<NB><<<n_r0, R0Shape<NB>::THREADS, R0Shape<NB>::SMEM, s>>>(rj, pd, F, FT, S, d);
+        r0_small_kernel<NB><<<std::min(n_r0, 3 * sms), R0Shape<NB>::THREADS, R0Shape<NB>::SMEM, s>>>(rj, n_r0, pd, F,
+                                                                                                 FT, S, d);
     finalize_small_kernel<8 * NB><<<n_cells, 256, 0, s>>>(cj, pd, F, FT, S, bases, W, d);
 }
 
@@ -842,14 +844,14 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
             noalloc_r0_jobs_kernel<<<(n_r0 + 255) / 256, 256, 0, s>>>(rj, cells, d, csize, per_cell);
         }
         switch (nb) {
-        case 1: noalloc_launch_diag<1>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 2: noalloc_launch_diag<2>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 3: noalloc_launch_diag<3>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 4: noalloc_launch_diag<4>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 5: noalloc_launch_diag<5>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 6: noalloc_launch_diag<6>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 7: noalloc_launch_diag<7>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        default: noalloc_launch_diag<8>(s, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 1: noalloc_launch_diag<1>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 2: noalloc_launch_diag<2>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 3: noalloc_launch_diag<3>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 4: noalloc_launch_diag<4>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 5: noalloc_launch_diag<5>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 6: noalloc_launch_diag<6>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 7: noalloc_launch_diag<7>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        default: noalloc_launch_diag<8>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
         }
     }
     gather_scores_kernel<<<1, 32, 0, s>>>(pdp, F, 1, dscore);

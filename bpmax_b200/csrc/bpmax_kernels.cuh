@@ -109,13 +109,23 @@ __global__ void single_strand_kernel(const PairDesc *__restrict__ pairs, const u
 //   R0 (V3/bpmax_verify.c:584-613):  max_{k1,k2} F(i1,k1,i2,k2) + F(k1+1,j1,k2+1,j2)
 //   R3 (:668-694):                    max_{k1}   S1(i1,k1) + F(k1+1,j1,i2,j2)
 //   R4 (:695-721):                    max_{k1}   F(i1,k1,i2,j2) + S1(k1+1,j1)
-// For one k1, R0 is a product of two upper-triangular matrices in the (max,+) semiring:
-//   C[i2][j2] = max_{k2} A[i2][k2] + B'[k2][j2],  A = F(i1,k1), B'[k2] = row k2+1 of F(k1+1,j1).
-// Shared memory holds A^T (from the FT copy) and B, both padded to a row stride of Np+4 floats.
-// The triangular product is split into tasks (bi,bj,kb): an 8x8 output micro-tile (bi,bj)
-// times one 8-wide k2 block kb, bi<=kb<=bj; every task is 8 k-steps of a 8x8 register tile,
-// so all threads do the same work. Tasks of one micro-tile live in different threads; their
-// partial maxima, like those of the CTAs that share the cell, merge by atomicMax into F.
+// Every finalized table F(a,b) stores S1(a,b) on its subdiagonal F[r][r-1] (never a logical
+// cell). With A = F(i1,k1) shifted one column right, A_s[i2][k'] = A[i2][k'-1] (A_s[0][0] =
+// S1(i1,k1)), and B = F(k1+1,j1) unshifted, one triangular (max,+) product gives all three:
+//   max_{k' in [i2, j2+1]} A_s[i2][k'] + B[k'][j2]
+//     k' = i2      : S1(i1,k1) + F(k1+1,j1)[i2][j2]                 (R3)
+//     i2 < k' <= j2: F(i1,k1)[i2][k'-1] + F(k1+1,j1)[k'][j2]         (R0, k2 = k'-1)
+//     k' = j2+1    : F(i1,k1)[i2][j2] + S1(k1+1,j1)                  (R4)
+// and every other k' meets a -inf. Shared memory holds A_s k'-major (A_s^T[k'][i2], rows 1..Np
+// copied from the FT table, row 0 = [S1(i1,k1), -inf...]) and B (rows 0..Np-1 of F, row Np =
+// -inf except B[Np][Np-1] = S1(k1+1,j1)); 16-byte chunks that hold only masked entries are never
+// copied (their shared slots stay -inf from the prologue), which halves the bytes per k1.
+// The product is split into tasks (bi,bj,kb): 8x8 output micro-tile (bi,bj) times k' block
+// [8kb, 8kb+8), bi<=kb<=bj, plus k' = 8bj+8 for the task with kb==bj. All tasks are 8 k-steps of
+// an 8x8 register tile (fp32 add + 3-input max per two candidates). Tasks of one micro-tile live
+// in different threads; their partial maxima, like those of the CTAs that share the cell, merge
+// by atomicMax into F. For Np=64 the shared rows are unpadded and XOR-swizzled per 16-byte chunk
+// and the task-to-lane table below makes every quarter-warp's 128-bit loads hit distinct banks.
 // ------------------------------------------------------------------------------------------
 struct R0Job {
     int pair, i1, k1a, k1b;  // cell (i1, i1+d) of pair, k1 in [k1a, k1b)
@@ -124,17 +134,46 @@ struct R0Job {
 template <int NB>
 struct R0Shape {
     static constexpr int NP = 8 * NB;
-    static constexpr int LD = NP + 4;                 // smem row stride (floats)
-    static constexpr int A_FLOATS = NP * LD;          // A^T[k2][i2]
-    static constexpr int B_FLOATS = (NP + 1) * LD;    // B[r][j2], r = 0..NP (row NP = -inf)
-    static constexpr int STAGE = A_FLOATS + B_FLOATS;
+    static constexpr bool SWZ = NB == 8;              // swizzled, unpadded rows
+    static constexpr int LD = SWZ ? NP : NP + 4;      // row stride (floats)
+    static constexpr int CPR = NP / 4;                // 16-byte chunks per row
+    static constexpr int ROWS = NP + 1;
+    static constexpr int A_FLOATS = ROWS * LD;        // A_s^T[k'][i2], k' = 0..NP
+    static constexpr int STAGE = 2 * A_FLOATS;        // + B[k'][j2], k' = 0..NP
     static constexpr int TASKS = NB * (NB + 1) * (NB + 2) / 6;
     static constexpr int THREADS = 128;
-    static constexpr int NSEG = (NP + 31) / 32;        // R3/R4 row segments per row
-    static constexpr int SEGW = NP / NSEG;             // segment width (a multiple of 4)
-    static constexpr int R34_THREADS = NP * NSEG;
-    static constexpr size_t SMEM = 2 * (size_t)STAGE * sizeof(float);
+    // two stages plus the chunk table (one 32-bit entry per copied 16-byte chunk, <= 2*NP*CPR)
+    static constexpr size_t SMEM = 2 * (size_t)STAGE * sizeof(float) + 2 * NP * CPR * sizeof(unsigned);
 };
+
+// shared offset (floats) of row r, column c (c a multiple of 4 for 16-byte accesses)
+template <int NB>
+__device__ __forceinline__ int r0_off(int r, int c)
+{
+    using Sh = R0Shape<NB>;
+    if constexpr (Sh::SWZ) {
+        const int cc = c >> 2;
+        const int pc = cc ^ (cc >> 3) ^ (((r >> 3) & 3) << 1);
+        return r * Sh::LD + (pc << 2) + (c & 3);
+    } else {
+        return r * Sh::LD + c;
+    }
+}
+
+// task (bi, bj, kb) of each lane for Np = 64: 15 quarter-warps whose 128-bit shared loads of A
+// and B hit 8 distinct bank groups (or one broadcast address) under r0_off's swizzle; lanes
+// 120..127 idle.
+__constant__ unsigned char c_r0_lane64[120][3] = {
+    {0,2,0},{0,6,0},{0,5,0},{0,4,0},{0,0,0},{0,1,0},{0,7,0},{0,3,0},{1,4,1},{0,5,1},{0,7,1},{0,4,1},
+    {0,6,1},{1,2,1},{1,7,1},{1,5,1},{0,2,2},{0,3,2},{2,5,2},{1,6,2},{1,5,2},{0,7,2},{1,2,2},{0,6,2},
+    {2,7,2},{0,4,2},{2,3,2},{1,4,2},{2,2,2},{2,4,2},{2,6,2},{1,7,2},{2,3,3},{2,7,3},{1,7,3},{3,5,3},
+    {3,7,3},{0,3,3},{1,4,3},{3,3,3},{2,5,3},{0,4,3},{0,7,3},{3,6,3},{2,6,3},{3,4,3},{2,4,3},{0,6,3},
+    {2,7,4},{2,5,4},{0,7,4},{0,5,4},{1,7,4},{1,4,4},{1,6,4},{3,7,4},{0,6,4},{0,4,4},{4,4,4},{2,6,4},
+    {3,4,4},{3,6,4},{2,4,4},{3,5,4},{5,6,5},{4,6,5},{2,7,5},{1,7,5},{5,7,5},{2,6,5},{1,6,5},{3,5,5},
+    {0,6,5},{5,5,5},{3,6,5},{0,5,5},{2,5,5},{3,7,5},{4,7,5},{0,7,5},{4,7,6},{6,6,6},{6,7,6},{0,7,6},
+    {0,6,6},{2,6,6},{3,6,6},{3,7,6},{0,7,7},{4,7,7},{3,7,7},{2,7,7},{1,7,7},{7,7,7},{5,7,7},{6,7,7},
+    {0,2,1},{0,3,1},{1,3,1},{1,1,1},{0,1,1},{1,6,1},{1,3,2},{1,6,3},{0,5,2},{4,6,4},{2,7,6},{1,6,6},
+    {1,7,6},{4,6,6},{5,6,6},{5,7,6},{1,3,3},{1,5,3},{0,5,3},{1,5,4},{4,5,4},{4,7,4},{1,5,5},{4,5,5}};
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
@@ -145,47 +184,54 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// number of 16-byte chunks copied per k1: A_s rows 1..NP need cc with 4cc <= r; B rows 0..NP-1
+// need cc with 4cc + 4 >= r (see r0_small_kernel)
+__host__ __device__ constexpr int r0_a_chunks(int NP, int r) { return (r / 4 + 1) < NP / 4 ? r / 4 + 1 : NP / 4; }
+__host__ __device__ constexpr int r0_b_first(int r) { return r <= 4 ? 0 : (r - 4 + 3) / 4; }
+
 template <int NB>
-__global__ void __launch_bounds__(128, 2)
-r0_small_kernel(const R0Job *__restrict__ jobs, const PairDesc *__restrict__ pairs, float *__restrict__ F,
-                const float *__restrict__ FT, const float *__restrict__ S, int d)
+__global__ void __launch_bounds__(128, 3)
+r0_small_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs,
+                float *__restrict__ F, const float *__restrict__ FT, const float *__restrict__ S, int d)
 {
     using Sh = R0Shape<NB>;
-    constexpr int NP = Sh::NP, LD = Sh::LD;
+    constexpr int NP = Sh::NP, CPR = Sh::CPR;
     extern __shared__ __align__(16) float smem[];
-    const R0Job job = jobs[blockIdx.x];
-    const PairDesc pd = pairs[job.pair];
-    const int M = pd.M, N = pd.N, i1 = job.i1, j1 = i1 + d;
-    const float *S1 = S + pd.S1_off;
-    const long long tile = (long long)NP * NP;
-    const float *Fp = F + pd.F_off;
-    const float *FTp = FT + pd.F_off;
+    // chunk table after the two stages: (A or B, source offset in the tile, shared offset in the stage)
+    unsigned *ctab = reinterpret_cast<unsigned *>(smem + 2 * Sh::STAGE);
     const int tid = threadIdx.x;
+    int jid = blockIdx.x;
+    if (jid >= njobs) return;
 
-    // row NP of B in both stages is -inf (B'[NP-1] beyond the table); never overwritten
-    for (int c = tid; c < LD; c += Sh::THREADS) {
-        smem[Sh::A_FLOATS + NP * LD + c] = NEG_INF;
-        smem[Sh::STAGE + Sh::A_FLOATS + NP * LD + c] = NEG_INF;
-    }
-
-    auto load_stage = [&](int stage, int k1) {
-        float *As = smem + stage * Sh::STAGE;
-        float *Bs = As + Sh::A_FLOATS;
-        const float *ga = FTp + cell_index(M, i1, k1) * tile;      // A^T = FT(i1,k1)
-        const float *gb = Fp + cell_index(M, k1 + 1, j1) * tile;   // B   = F(k1+1,j1)
-        constexpr int CPR = NP / 4;                                 // 16-byte chunks per row
-        for (int q = tid; q < 2 * NP * CPR; q += Sh::THREADS) {
-            const int which = q / (NP * CPR), rr = (q / CPR) % NP, cc = (q % CPR) * 4;
-            if (which == 0) cp_async16(As + rr * LD + cc, ga + rr * NP + cc);
-            else cp_async16(Bs + rr * LD + cc, gb + rr * NP + cc);
+    // prologue (once per CTA): every shared slot -inf; chunks that only hold masked entries are
+    // never copied, so their slots stay -inf for every job
+    for (int q = tid * 4; q < 2 * Sh::STAGE; q += Sh::THREADS * 4)
+        *reinterpret_cast<float4 *>(smem + q) = make_float4(NEG_INF, NEG_INF, NEG_INF, NEG_INF);
+    int nchunks = 0;
+    for (int r = 1; r <= NP; ++r) nchunks += r0_a_chunks(NP, r);
+    for (int r = 0; r < NP; ++r) nchunks += CPR - r0_b_first(r);
+    if (tid < 2 * NP) {  // one thread per copied row builds that row's entries
+        int base = 0;
+        const bool isA = tid < NP;
+        const int row = isA ? tid + 1 : tid - NP;
+        for (int r = 1; r <= (isA ? row - 1 : NP); ++r) base += r0_a_chunks(NP, r);
+        if (!isA)
+            for (int r = 0; r < row; ++r) base += CPR - r0_b_first(r);
+        const int c0 = isA ? 0 : r0_b_first(row), c1 = isA ? r0_a_chunks(NP, row) : CPR;
+        for (int cc = c0; cc < c1; ++cc) {
+            const unsigned src = isA ? (row - 1) * NP + 4 * cc : row * NP + 4 * cc;
+            const unsigned dst = (isA ? 0 : Sh::A_FLOATS) + r0_off<NB>(row, 4 * cc);
+            ctab[base++] = (src << 16) | dst;
         }
-        cp_async_commit();
-    };
+    }
+    __syncthreads();
 
-    // task of this thread: micro-tile (bi,bj), k-block kb
+    const long long tile = (long long)NP * NP;
     int bi = 0, bj = 0, kb = 0;
     const bool has_task = tid < Sh::TASKS;
-    {
+    if constexpr (Sh::SWZ) {
+        if (has_task) { bi = c_r0_lane64[tid][0]; bj = c_r0_lane64[tid][1]; kb = c_r0_lane64[tid][2]; }
+    } else {
         int t = tid, found = 0;
         for (int a = 0; a < NB && !found; ++a)
             for (int b = a; b < NB && !found; ++b) {
@@ -194,40 +240,61 @@ r0_small_kernel(const R0Job *__restrict__ jobs, const PairDesc *__restrict__ pai
                 else t -= n;
             }
     }
-    // R3/R4 ownership: row r of B (R3 cells (r, c..c+SEGW)), row r of A^T (R4 cells (c.., r))
-    const bool has34 = tid < Sh::R34_THREADS;
-    const int r34 = tid / Sh::NSEG, c34 = (tid % Sh::NSEG) * Sh::SEGW;
+    const bool edge = has_task && kb == bj;
+
+    // issues the copies of (job, k1) into stage
+    auto load_stage = [&](int stage, const R0Job &jb, int k1) {
+        const PairDesc pd = pairs[jb.pair];
+        const int M = pd.M, j1 = jb.i1 + d;
+        float *st = smem + stage * Sh::STAGE;
+        const float *ga = FT + pd.F_off + cell_index(M, jb.i1, k1) * tile;  // column k of F(i1,k1)
+        const float *gb = F + pd.F_off + cell_index(M, k1 + 1, j1) * tile;  // F(k1+1,j1)
+        for (int e = tid; e < nchunks; e += Sh::THREADS) {
+            const unsigned v = ctab[e];
+            const unsigned dst = v & 0xffffu, src = v >> 16;
+            cp_async16(st + dst, (dst < (unsigned)Sh::A_FLOATS ? ga : gb) + src);
+        }
+        cp_async_commit();
+        const float *S1 = S + pd.S1_off;
+        if (tid == 0) st[r0_off<NB>(0, 0)] = S1[jb.i1 * M + k1];                               // R3 slot of i2 = 0
+        if (tid == 1) st[Sh::A_FLOATS + r0_off<NB>(NP, NP - 4) + 3] = S1[(k1 + 1) * M + j1];  // R4 slot of j2 = NP-1
+    };
 
     float acc[8][8];
-    float acc3[Sh::SEGW], acc4[Sh::SEGW];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc[i][j] = NEG_INF;
-#pragma unroll
-    for (int i = 0; i < Sh::SEGW; ++i) { acc3[i] = NEG_INF; acc4[i] = NEG_INF; }
 
-    load_stage(0, job.k1a);
-    for (int k1 = job.k1a; k1 < job.k1b; ++k1) {
-        const int stage = (k1 - job.k1a) & 1;
-        if (k1 + 1 < job.k1b) { load_stage(stage ^ 1, k1 + 1); cp_async_wait<1>(); }
+    R0Job job = jobs[jid];
+    int k1 = job.k1a, stage = 0;
+    load_stage(0, job, k1);
+    while (true) {
+        // the next (job, k1) item of this CTA, possibly in its next job
+        R0Job njob = job;
+        int njid = jid, nk1 = k1 + 1;
+        if (nk1 >= job.k1b) {
+            njid = jid + gridDim.x;
+            if (njid < njobs) { njob = jobs[njid]; nk1 = njob.k1a; }
+        }
+        const bool has_next = njid < njobs;
+        if (has_next) { load_stage(stage ^ 1, njob, nk1); cp_async_wait<1>(); }
         else cp_async_wait<0>();
         __syncthreads();
         const float *As = smem + stage * Sh::STAGE;
         const float *Bs = As + Sh::A_FLOATS;
         if (has_task) {
-            const float *pa = As + (8 * kb) * LD + 8 * bi;
-            const float *pb = Bs + (8 * kb + 1) * LD + 8 * bj;
 #pragma unroll
             for (int k = 0; k < 8; k += 2) {
-                const float4 a0 = *reinterpret_cast<const float4 *>(pa + k * LD);
-                const float4 a1 = *reinterpret_cast<const float4 *>(pa + k * LD + 4);
-                const float4 a2 = *reinterpret_cast<const float4 *>(pa + (k + 1) * LD);
-                const float4 a3 = *reinterpret_cast<const float4 *>(pa + (k + 1) * LD + 4);
-                const float4 b0 = *reinterpret_cast<const float4 *>(pb + k * LD);
-                const float4 b1 = *reinterpret_cast<const float4 *>(pb + k * LD + 4);
-                const float4 b2 = *reinterpret_cast<const float4 *>(pb + (k + 1) * LD);
-                const float4 b3 = *reinterpret_cast<const float4 *>(pb + (k + 1) * LD + 4);
+                const int r = 8 * kb + k;
+                const float4 a0 = *reinterpret_cast<const float4 *>(As + r0_off<NB>(r, 8 * bi));
+                const float4 a1 = *reinterpret_cast<const float4 *>(As + r0_off<NB>(r, 8 * bi + 4));
+                const float4 a2 = *reinterpret_cast<const float4 *>(As + r0_off<NB>(r + 1, 8 * bi));
+                const float4 a3 = *reinterpret_cast<const float4 *>(As + r0_off<NB>(r + 1, 8 * bi + 4));
+                const float4 b0 = *reinterpret_cast<const float4 *>(Bs + r0_off<NB>(r, 8 * bj));
+                const float4 b1 = *reinterpret_cast<const float4 *>(Bs + r0_off<NB>(r, 8 * bj + 4));
+                const float4 b2 = *reinterpret_cast<const float4 *>(Bs + r0_off<NB>(r + 1, 8 * bj));
+                const float4 b3 = *reinterpret_cast<const float4 *>(Bs + r0_off<NB>(r + 1, 8 * bj + 4));
                 const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
                 const float aw[8] = {a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
                 const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
@@ -237,45 +304,36 @@ r0_small_kernel(const R0Job *__restrict__ jobs, const PairDesc *__restrict__ pai
 #pragma unroll
                     for (int j = 0; j < 8; ++j) acc[i][j] = fmax3(acc[i][j], av[i] + bv[j], aw[i] + bw[j]);
             }
-        }
-        if (has34) {
-            const float s1a = S1[i1 * M + k1], s1b = S1[(k1 + 1) * M + j1];
-            const float *rb = Bs + r34 * LD + c34;  // F(k1+1,j1)[r34][c34 + x]
-            const float *ra = As + r34 * LD + c34;  // F(i1,k1)[c34 + x][r34]
+            if (edge) {  // k' = 8bj+8: R4 of column j2 = 8bj+7
+                const int r = 8 * bj + 8;
+                const float4 a0 = *reinterpret_cast<const float4 *>(As + r0_off<NB>(r, 8 * bi));
+                const float4 a1 = *reinterpret_cast<const float4 *>(As + r0_off<NB>(r, 8 * bi + 4));
+                const float bs = Bs[r0_off<NB>(r, 8 * bj + 4) + 3];
+                const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
 #pragma unroll
-            for (int x = 0; x < Sh::SEGW; x += 4) {
-                const float4 vb = *reinterpret_cast<const float4 *>(rb + x);
-                const float4 va = *reinterpret_cast<const float4 *>(ra + x);
-                acc3[x + 0] = fmaxf(acc3[x + 0], s1a + vb.x);
-                acc3[x + 1] = fmaxf(acc3[x + 1], s1a + vb.y);
-                acc3[x + 2] = fmaxf(acc3[x + 2], s1a + vb.z);
-                acc3[x + 3] = fmaxf(acc3[x + 3], s1a + vb.w);
-                acc4[x + 0] = fmaxf(acc4[x + 0], va.x + s1b);
-                acc4[x + 1] = fmaxf(acc4[x + 1], va.y + s1b);
-                acc4[x + 2] = fmaxf(acc4[x + 2], va.z + s1b);
-                acc4[x + 3] = fmaxf(acc4[x + 3], va.w + s1b);
+                for (int i = 0; i < 8; ++i) acc[i][7] = fmaxf(acc[i][7], av[i] + bs);
             }
         }
         __syncthreads();
-    }
-
-    int *out = reinterpret_cast<int *>(F + pd.F_off + cell_index(M, i1, j1) * tile);
-    if (has_task) {
+        if (njid != jid || !has_next) {  // job done: merge its partial maxima into F(i1, i1+d)
+            if (has_task) {
+                const PairDesc pd = pairs[job.pair];
+                int *out = reinterpret_cast<int *>(F + pd.F_off + cell_index(pd.M, job.i1, job.i1 + d) * tile);
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+                for (int i = 0; i < 8; ++i)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int i2 = 8 * bi + i, j2 = 8 * bj + j;
-                if (i2 < j2 && j2 < N) atomicMax(out + i2 * NP + j2, __float_as_int(acc[i][j]));
+                    for (int j = 0; j < 8; ++j) {
+                        const int i2 = 8 * bi + i, j2 = 8 * bj + j;
+                        if (i2 <= j2 && j2 < pd.N) atomicMax(out + i2 * NP + j2, __float_as_int(acc[i][j]));
+                        acc[i][j] = NEG_INF;
+                    }
             }
-    }
-    if (has34) {
-#pragma unroll
-        for (int x = 0; x < Sh::SEGW; ++x) {
-            const int c = c34 + x;
-            if (r34 <= c && c < N) atomicMax(out + r34 * NP + c, __float_as_int(acc3[x]));  // R3 at (r34, c)
-            if (c <= r34 && r34 < N) atomicMax(out + c * NP + r34, __float_as_int(acc4[x]));  // R4 at (c, r34)
         }
+        if (!has_next) break;
+        jid = njid;
+        job = njob;
+        k1 = nk1;
+        stage ^= 1;
     }
 }
 
@@ -360,6 +418,9 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restri
         }
         __syncthreads();
     }
+    // S1(i1,j1) on the subdiagonal: the R3/R4 slots of the product kernel (never a logical cell)
+    for (int r = 1 + tid; r < NP; r += nt) Fs[r * LD + r - 1] = s1v;
+    __syncthreads();
     for (int q = tid; q < NP * NP; q += nt) {
         const int r = q / NP, c = q % NP;
         Fc[q] = Fs[r * LD + c];
