@@ -41,7 +41,7 @@ struct Plan {
     int bases_bytes = 0;
     int maxM = 0;
     // per diagonal and Np class (index NB-1): ranges in the job arrays
-    struct Launch { int d, nb, first, count; };
+    struct Launch { int d, nb, first, count, s1_first = 0, s1_count = 0; };
     std::vector<Launch> r0_launches, fin_launches;
     std::vector<R0Job> r0_jobs;
     std::vector<CellJob> cell_jobs;
@@ -169,6 +169,10 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
             P.r0_launches.push_back(rl);
         }
     }
+    // S1 of diagonal d+1 is computed by the finalize launch of diagonal d (same Np class)
+    for (auto &fl : P.fin_launches)
+        for (const auto &nx : P.fin_launches)
+            if (nx.d == fl.d + 1 && nx.nb == fl.nb) { fl.s1_first = nx.first; fl.s1_count = nx.count; }
     return BPMAX_OK;
 }
 
@@ -185,9 +189,10 @@ void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L)
 template <int NB>
 void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L)
 {
-    finalize_small_kernel<8 * NB><<<L.count, 256, 0, ctx->stream>>>(
-        (const CellJob *)ctx->celljobs.p + L.first, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
-        (float *)ctx->FT.p, (const float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W, L.d);
+    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, 0, ctx->stream>>>(
+        (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
+        (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
+        (const uint8_t *)ctx->bases.p, ctx->W, L.d);
 }
 
 template <int NB>
@@ -230,9 +235,10 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
 {
     long launches = 0;
     CK(cudaMemsetAsync(ctx->F.p, 0, (size_t)P.F_floats * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->S.p, 0, (size_t)P.S_floats * sizeof(float), ctx->stream));  // S1 starts at 0
     {
         ProfScope ps(ctx, kp, 0);
-        single_strand_kernel<<<2 * (int)P.pairs.size(), 512, 0, ctx->stream>>>(
+        single_strand_kernel<<<(int)P.pairs.size(), 512, 0, ctx->stream>>>(
             (const PairDesc *)ctx->pairs.p, (const uint8_t *)ctx->bases.p, (float *)ctx->S.p, ctx->W);
     }
     ++launches;
@@ -761,7 +767,9 @@ void noalloc_launch_diag(cudaStream_t s, int sms, int d, int n_r0, int n_cells, 
     if (d > 0)
         r0_small_kernel<NB><<<std::min(n_r0, 3 * sms), R0Shape<NB>::THREADS, R0Shape<NB>::SMEM, s>>>(rj, n_r0, pd, F,
                                                                                                  FT, S, d);
-    finalize_small_kernel<8 * NB><<<n_cells, 256, 0, s>>>(cj, pd, F, FT, S, bases, W, d);
+    const int n_s1 = n_cells - 1;  // S1 cells of diagonal d+1: the first n_cells-1 entries of cj
+    finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + 3) / 4, 128, 0, s>>>(cj, n_cells, cj, n_s1, pd, F, FT, S, bases,
+                                                                          W, d);
 }
 
 }  // namespace
@@ -827,12 +835,13 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     if (!ok(cudaMemcpyAsync(seqs, seq1, sizeof(int) * M, cudaMemcpyHostToDevice, s)) ||
         !ok(cudaMemcpyAsync(seqs + M, seq2, sizeof(int) * N, cudaMemcpyHostToDevice, s)) ||
         !ok(cudaMemcpyAsync(pdp, &pd, sizeof pd, cudaMemcpyHostToDevice, s)) ||
-        !ok(cudaMemsetAsync(F, 0, sizeof(float) * nF, s))) {  // F starts at +0 on every call
+        !ok(cudaMemsetAsync(F, 0, sizeof(float) * nF, s)) ||  // F starts at +0 on every call
+        !ok(cudaMemsetAsync(S, 0, sizeof(float) * S2_rel, s))) {  // and S1 at 0
         cudaGetLastError();
         return BPMAX_ECUDA;
     }
     noalloc_prep_kernel<<<8, 256, 0, s>>>(seqs, (int)M, (int)N, bases, cj);
-    single_strand_kernel<<<2, 512, 0, s>>>(pdp, bases, S, W);
+    single_strand_kernel<<<1, 512, 0, s>>>(pdp, bases, S, W);
     for (int d = 0; d < (int)M; ++d) {
         const int cells = (int)M - d;
         int n_r0 = 0;

@@ -63,16 +63,16 @@ __host__ __device__ __forceinline__ long long cell_index(int M, int i1, int j1)
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
 
 // ------------------------------------------------------------------------------------------
-// Single-strand table (V3/bpmax_verify.c:533-544 for S1, :560-571 for S2 over the reversed
-// strand): S(i,j) = 0 if j-i<=3, else max(S(i+1,j-1)+intra(s[i],s[j]), max_{i<=k<j} S(i,k)+S(k+1,j)).
-// One CTA per (pair, strand); wavefront over the diagonal j-i. Cells of S2 outside the N x N
-// upper triangle are left at 0 and never read.
+// Single-strand table S2 over the reversed strand 2 (V3/bpmax_verify.c:560-571):
+// S(i,j) = 0 if j-i<=3, else max(S(i+1,j-1)+intra(s[i],s[j]), max_{i<=k<j} S(i,k)+S(k+1,j)).
+// One CTA per pair; wavefront over the diagonal j-i. Cells outside the N x N upper triangle are
+// left at 0 and never read. (S1 is built diagonal by diagonal inside finalize_small_kernel.)
 // ------------------------------------------------------------------------------------------
 __global__ void single_strand_kernel(const PairDesc *__restrict__ pairs, const uint8_t *__restrict__ bases,
                                      float *__restrict__ S, Weights W)
 {
-    const PairDesc pd = pairs[blockIdx.x >> 1];
-    const bool second = blockIdx.x & 1;
+    const PairDesc pd = pairs[blockIdx.x];
+    const bool second = true;
     const int L = second ? pd.N : pd.M;
     const int ld = second ? pd.Np : pd.M;
     const uint8_t *s = bases + (second ? pd.seq2_off : pd.seq1_off);
@@ -180,6 +180,11 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
@@ -254,10 +259,10 @@ r0_small_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__res
             const unsigned dst = v & 0xffffu, src = v >> 16;
             cp_async16(st + dst, (dst < (unsigned)Sh::A_FLOATS ? ga : gb) + src);
         }
-        cp_async_commit();
         const float *S1 = S + pd.S1_off;
-        if (tid == 0) st[r0_off<NB>(0, 0)] = S1[jb.i1 * M + k1];                               // R3 slot of i2 = 0
-        if (tid == 1) st[Sh::A_FLOATS + r0_off<NB>(NP, NP - 4) + 3] = S1[(k1 + 1) * M + j1];  // R4 slot of j2 = NP-1
+        if (tid == 0) cp_async4(st + r0_off<NB>(0, 0), S1 + jb.i1 * M + k1);                               // R3 slot, i2 = 0
+        if (tid == 1) cp_async4(st + Sh::A_FLOATS + r0_off<NB>(NP, NP - 4) + 3, S1 + (k1 + 1) * M + j1);  // R4 slot, j2 = NP-1
+        cp_async_commit();
     };
 
     float acc[8][8];
@@ -278,9 +283,11 @@ r0_small_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__res
             if (njid < njobs) { njob = jobs[njid]; nk1 = njob.k1a; }
         }
         const bool has_next = njid < njobs;
-        if (has_next) { load_stage(stage ^ 1, njob, nk1); cp_async_wait<1>(); }
-        else cp_async_wait<0>();
+        cp_async_wait<0>();
+        // one barrier per item: it publishes this stage's copies and guarantees every thread has
+        // finished the previous item, whose stage the next copies overwrite
         __syncthreads();
+        if (has_next) load_stage(stage ^ 1, njob, nk1);
         const float *As = smem + stage * Sh::STAGE;
         const float *Bs = As + Sh::A_FLOATS;
         if (has_task) {
@@ -314,7 +321,6 @@ r0_small_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__res
                 for (int i = 0; i < 8; ++i) acc[i][7] = fmaxf(acc[i][7], av[i] + bs);
             }
         }
-        __syncthreads();
         if (njid != jid || !has_next) {  // job done: merge its partial maxima into F(i1, i1+d)
             if (has_task) {
                 const PairDesc pd = pairs[job.pair];
@@ -338,29 +344,56 @@ r0_small_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__res
 }
 
 // ------------------------------------------------------------------------------------------
-// Finalize one outer cell (one CTA per cell of diagonal d, Np <= 64): adds the candidates that
+// Finalize the outer cells of diagonal d (Np <= 64; 4 warps per cell): adds the candidates that
 // do not come from R0/R3/R4 and runs the inner wavefront of R1/R2/SW2 in shared memory.
 //   base  i1==j1 && i2==j2: inter(s1[i1], s2r[i2])            (assignment, eval_FTable :576)
-//   S1(i1,j1)+S2(i2,j2); SW1 = F(i1+1,j1-1,i2,j2)+intra(s1[i1],s1[j1]) if j1-i1>=4
+//   S1(i1,j1)+S2(i2,j2)
 //   SW2 = F(i1,j1,i2+1,j2-1)+intra(s2r[i2],s2r[j2]) if j2-i2>=4
 //   R1 (:614-640) max_{k2} F(i1,j1,i2,k2)+S2(k2+1,j2); R2 (:641-667) max_{k2} S2(i2,k2)+F(i1,j1,k2+1,j2)
-// F arrives holding max(R0,R3,R4) (or 0 on a cleared cell); all literal-0 candidates are
-// covered because every value is >= +0. Writes F and FT, -inf outside the logical triangle.
+// F arrives holding max(R0,R3,R4,SW1) (or +0): SW1 = F(i1+1,j1-1,.)+intra(s1[i1],s1[j1])
+// (V3/bpmax_outer_south_west.c:115-160) was stored into this cell's still-cleared table by the
+// finalize of (i1+1, j1-1) two diagonals earlier, before any product touched it. Every literal-0
+// candidate is covered because every value is >= +0. Writes F and FT: -inf outside the logical
+// triangle and S1(i1,j1) on the subdiagonal (the R3/R4 slots of the product kernel).
+// CTAs after the first njobs compute S1 on diagonal d+1 (V3/bpmax_verify.c:533-544), one warp
+// per cell, from S1 diagonals <= d (S1 is cleared to 0 before the fill; j-i <= 3 stays 0).
 // ------------------------------------------------------------------------------------------
 struct CellJob {
     int pair, i1;
 };
 
 template <int NP>
-__global__ void __launch_bounds__(256)
-finalize_small_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restrict__ pairs,
-                      float *__restrict__ F, float *__restrict__ FT, const float *__restrict__ S,
-                      const uint8_t *__restrict__ bases, Weights W, int d)
+__global__ void __launch_bounds__(128)
+finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
+                      const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
+                      float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
 {
-    constexpr int LD = NP + 1;
-    __shared__ float Fs[NP * LD];
-    __shared__ float Ss[(NP + 1) * LD];
+    constexpr int LD = NP + 4;  // 16-byte rows; odd multiple of 4 words per row keeps column walks conflict-free
+    __shared__ __align__(16) float Fs[NP * LD];
+    __shared__ __align__(16) float Ss[NP * LD];
     __shared__ uint8_t sb[NP];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if ((int)blockIdx.x >= njobs) {  // S1 cells (i, i+d+1), one per warp
+        const int q = ((int)blockIdx.x - njobs) * 4 + warp;
+        if (q >= ns1) return;
+        const CellJob job = s1jobs[q];
+        const PairDesc pd = pairs[job.pair];
+        const int M = pd.M, i = job.i1, j = i + d + 1;
+        float *S1 = S + pd.S1_off;
+        if (j - i <= 3) return;  // stays 0
+        const uint8_t *s1 = bases + pd.seq1_off;
+        float r0 = NEG_INF, r1 = NEG_INF;
+        int k = i + lane;
+        for (; k + 32 < j; k += 64) {
+            r0 = fmaxf(r0, S1[i * M + k] + S1[(k + 1) * M + j]);
+            r1 = fmaxf(r1, S1[i * M + k + 32] + S1[(k + 33) * M + j]);
+        }
+        if (k < j) r0 = fmaxf(r0, S1[i * M + k] + S1[(k + 1) * M + j]);
+        float red = fmaxf(r0, r1);
+        for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
+        if (lane == 0) S1[i * M + j] = fmaxf(S1[(i + 1) * M + (j - 1)] + score_w(W.w, s1[i], s1[j]), red);
+        return;
+    }
     const CellJob job = jobs[blockIdx.x];
     const PairDesc pd = pairs[job.pair];
     const int M = pd.M, N = pd.N, i1 = job.i1, j1 = i1 + d;
@@ -371,27 +404,24 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restri
     const float *S2 = S + pd.S2_off;
     const uint8_t *s1 = bases + pd.seq1_off;
     const uint8_t *s2r = bases + pd.seq2_off;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const float s1v = S1[i1 * M + j1];
-    const bool sw1 = d >= 4;
-    const float w1 = sw1 ? score_w(W.w, s1[i1], s1[j1]) : 0.0f;
-    const float *Fsw = sw1 ? F + pd.F_off + cell_index(M, i1 + 1, j1 - 1) * tile : nullptr;
-
-    for (int q = tid; q < NP; q += nt) sb[q] = q < N ? s2r[q] : 4;
-    for (int q = tid; q < (NP + 1) * LD; q += nt) {
-        const int r = q / LD, c = q % LD;
-        Ss[q] = (r < N && c < N) ? S2[r * NP + c] : 0.0f;
+    constexpr int CPR = NP / 4;
+    for (int q = tid; q < 2 * NP * CPR; q += 128) {
+        const int which = q / (NP * CPR), r = (q / CPR) % NP, c = (q % CPR) * 4;
+        if (which == 0) cp_async16(Fs + r * LD + c, Fc + r * NP + c);
+        else cp_async16(Ss + r * LD + c, S2 + r * NP + c);
     }
-    for (int q = tid; q < NP * NP; q += nt) {
+    cp_async_commit();
+    for (int q = tid; q < NP; q += 128) sb[q] = q < N ? s2r[q] : 4;
+    const float s1v = S1[i1 * M + j1];
+    cp_async_wait<0>();
+    __syncthreads();
+    // init candidates
+    for (int q = tid; q < NP * NP; q += 128) {
         const int r = q / NP, c = q % NP;
         float v = NEG_INF;
         if (r <= c && c < N) {
-            if (d == 0 && r == c) {
-                v = score_w(W.w + 6, s1[i1], s2r[r]);
-            } else {
-                v = fmaxf(Fc[q], s1v + S2[r * NP + c]);
-                if (sw1) v = fmaxf(v, Fsw[q] + w1);
-            }
+            if (d == 0 && r == c) v = score_w(W.w + 6, s1[i1], sb[r]);
+            else v = fmaxf(Fs[r * LD + c], s1v + Ss[r * LD + c]);
         }
         Fs[r * LD + c] = v;
     }
@@ -399,16 +429,23 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restri
     for (int dd = 1; dd < N; ++dd) {
         const int cells = N - dd;
         int g = 1;
-        while (g < 32 && g * 2 * cells <= nt) g *= 2;
+        while (g < 32 && g * 2 * cells <= 128) g *= 2;
         const int lane_g = tid & (g - 1);
-        const int slots = nt / g;
+        const int slots = 128 / g;
         for (int base = 0; base < cells; base += slots) {
             const int i2 = base + tid / g, j2 = i2 + dd;
             const bool act = i2 < cells;
-            float red = NEG_INF;
-            if (act)
-                for (int k = i2 + lane_g; k < j2; k += g)
-                    red = fmax3(red, Fs[i2 * LD + k] + Ss[(k + 1) * LD + j2], Ss[i2 * LD + k] + Fs[(k + 1) * LD + j2]);
+            float r0 = NEG_INF, r1 = NEG_INF;
+            if (act) {
+                int k = i2 + lane_g;
+                for (; k + g < j2; k += 2 * g) {
+                    r0 = fmax3(r0, Fs[i2 * LD + k] + Ss[(k + 1) * LD + j2], Ss[i2 * LD + k] + Fs[(k + 1) * LD + j2]);
+                    r1 = fmax3(r1, Fs[i2 * LD + k + g] + Ss[(k + g + 1) * LD + j2],
+                               Ss[i2 * LD + k + g] + Fs[(k + g + 1) * LD + j2]);
+                }
+                if (k < j2) r0 = fmax3(r0, Fs[i2 * LD + k] + Ss[(k + 1) * LD + j2], Ss[i2 * LD + k] + Fs[(k + 1) * LD + j2]);
+            }
+            float red = fmaxf(r0, r1);
             for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
             if (act && lane_g == 0) {
                 float v = fmaxf(Fs[i2 * LD + j2], red);
@@ -418,13 +455,31 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restri
         }
         __syncthreads();
     }
-    // S1(i1,j1) on the subdiagonal: the R3/R4 slots of the product kernel (never a logical cell)
-    for (int r = 1 + tid; r < NP; r += nt) Fs[r * LD + r - 1] = s1v;
+    // SW1 candidate of cell (i1-1, j1+1), whose table nothing else has written yet
+    const bool push = i1 >= 1 && j1 + 1 < M && d + 2 >= 4;
+    const float wp = push ? score_w(W.w, s1[i1 - 1], s1[j1 + 1]) : 0.0f;
+    float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * tile : nullptr;
+    for (int q4 = tid; q4 < NP * NP / 4; q4 += 128) {
+        const int r = (4 * q4) / NP, c = (4 * q4) % NP;
+        const float4 v = *reinterpret_cast<const float4 *>(Fs + r * LD + c);
+        if (push) {
+            float4 u;
+            u.x = (r <= c + 0 && c + 0 < N) ? v.x + wp : 0.0f;
+            u.y = (r <= c + 1 && c + 1 < N) ? v.y + wp : 0.0f;
+            u.z = (r <= c + 2 && c + 2 < N) ? v.z + wp : 0.0f;
+            u.w = (r <= c + 3 && c + 3 < N) ? v.w + wp : 0.0f;
+            *reinterpret_cast<float4 *>(Fn + 4 * q4) = u;
+        }
+    }
     __syncthreads();
-    for (int q = tid; q < NP * NP; q += nt) {
-        const int r = q / NP, c = q % NP;
-        Fc[q] = Fs[r * LD + c];
-        FTc[q] = Fs[c * LD + r];
+    // S1(i1,j1) on the subdiagonal: the R3/R4 slots of the product kernel (never a logical cell)
+    for (int r = 1 + tid; r < NP; r += 128) Fs[r * LD + r - 1] = s1v;
+    __syncthreads();
+    for (int q4 = tid; q4 < NP * NP / 4; q4 += 128) {
+        const int r = (4 * q4) / NP, c = (4 * q4) % NP;
+        *reinterpret_cast<float4 *>(Fc + 4 * q4) = *reinterpret_cast<const float4 *>(Fs + r * LD + c);
+        *reinterpret_cast<float4 *>(FTc + 4 * q4) =
+            make_float4(Fs[c * LD + r], Fs[(c + 1) * LD + r], Fs[(c + 2) * LD + r], Fs[(c + 3) * LD + r]);
     }
 }
 
