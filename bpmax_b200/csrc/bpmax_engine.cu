@@ -22,12 +22,17 @@
 
 #include "../../include/bpmax_gpu.h"
 #include "bpmax_kernels.cuh"
+#include "bpmax_kernels_large.cuh"
 
 using namespace bpmax;
 
 namespace {
 
 constexpr int MAX_SMALL_NP = 64;
+constexpr int MAX_NP = 4096;
+
+// inner table width of a strand-2 length: multiples of 8 up to 64, then multiples of 64
+int padded_width(int N) { return N <= MAX_SMALL_NP ? std::max(8, (N + 7) / 8 * 8) : (N + 63) / 64 * 64; }
 
 struct DevBuf {
     void *p = nullptr;
@@ -41,9 +46,10 @@ struct Plan {
     int bases_bytes = 0;
     int maxM = 0;
     // per diagonal and Np class (index NB-1): ranges in the job arrays
-    struct Launch { int d, nb, first, count, s1_first = 0, s1_count = 0; };
+    struct Launch { int d, np, first, count, s1_first = 0, s1_count = 0; };  // np = inner table width class
     std::vector<Launch> r0_launches, fin_launches;
     std::vector<R0Job> r0_jobs;
+    std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > 64 (first/count index this array)
     std::vector<CellJob> cell_jobs;
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
@@ -58,7 +64,7 @@ struct bpmax_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
     std::string err;
-    DevBuf F, FT, S, bases, pairs, r0jobs, celljobs, scores, conv;
+    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv;
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -123,15 +129,20 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         PairDesc pd{};
         pd.M = Ms[p];
         pd.N = Ns[p];
-        pd.Np = std::max(8, (Ns[p] + 7) / 8 * 8);
-        if (pd.Np > MAX_SMALL_NP)
-            return fail(ctx, BPMAX_EINVAL, "strand-2 length %d > %d is not supported by this build", Ns[p], MAX_SMALL_NP);
+        pd.Np = padded_width(Ns[p]);
+        if (pd.Np > MAX_NP) return fail(ctx, BPMAX_EINVAL, "strand-2 length %d > %d is not supported", Ns[p], MAX_NP);
         pd.F_off = f;
         f = align64(f + (long long)Ms[p] * (Ms[p] + 1) / 2 * pd.Np * pd.Np);
         pd.S1_off = s;
         s = align64(s + (long long)Ms[p] * Ms[p]);
         pd.S2_off = s;
         s = align64(s + (long long)pd.Np * pd.Np);
+        if (pd.Np > MAX_SMALL_NP) {
+            pd.S2m_off = s;
+            s = align64(s + (long long)pd.Np * pd.Np);
+            pd.S2t_off = s;
+            s = align64(s + (long long)pd.Np * pd.Np);
+        }
         pd.seq1_off = b;
         b += Ms[p];
         pd.seq2_off = b;
@@ -142,38 +153,71 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     P.F_floats = f;
     P.S_floats = s;
     P.bases_bytes = b;
-    // jobs, grouped by diagonal then Np class
+    std::vector<int> classes;
+    for (const auto &pd : P.pairs) classes.push_back(pd.Np);
+    std::sort(classes.begin(), classes.end());
+    classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    // jobs, grouped by diagonal then inner width class
     const int target = 4 * ctx->sms;  // CTAs per diagonal launch worth splitting k1 for
     for (int d = 0; d < P.maxM; ++d) {
-        for (int nb = 1; nb <= MAX_SMALL_NP / 8; ++nb) {
+        for (int np : classes) {
             long long cells = 0;
             for (int p = 0; p < n; ++p)
-                if (P.pairs[p].Np == 8 * nb && Ms[p] > d) cells += Ms[p] - d;
+                if (P.pairs[p].Np == np && Ms[p] > d) cells += Ms[p] - d;
             if (cells == 0) continue;
-            Plan::Launch fl{d, nb, (int)P.cell_jobs.size(), 0};
+            Plan::Launch fl{d, np, (int)P.cell_jobs.size(), 0};
             for (int p = 0; p < n; ++p)
-                if (P.pairs[p].Np == 8 * nb && Ms[p] > d)
+                if (P.pairs[p].Np == np && Ms[p] > d)
                     for (int i1 = 0; i1 < Ms[p] - d; ++i1) P.cell_jobs.push_back(CellJob{p, i1});
             fl.count = (int)P.cell_jobs.size() - fl.first;
             P.fin_launches.push_back(fl);
             if (d == 0) continue;
-            long long chunks = std::max(1LL, std::min((long long)d, (target + cells - 1) / cells));
+            const bool large = np > MAX_SMALL_NP;
+            const int nbk = np / 64;
+            const long long units = large ? cells * (nbk * (nbk + 1) / 2) : cells;
+            long long chunks = std::max(1LL, std::min((long long)d, (target + units - 1) / units));
             int csize = (int)((d + chunks - 1) / chunks);
-            Plan::Launch rl{d, nb, (int)P.r0_jobs.size(), 0};
+            Plan::Launch rl{d, np, large ? (int)P.r0l_jobs.size() : (int)P.r0_jobs.size(), 0};
             for (int p = 0; p < n; ++p)
-                if (P.pairs[p].Np == 8 * nb && Ms[p] > d)
+                if (P.pairs[p].Np == np && Ms[p] > d)
                     for (int i1 = 0; i1 < Ms[p] - d; ++i1)
-                        for (int k = i1; k < i1 + d; k += csize)
-                            P.r0_jobs.push_back(R0Job{p, i1, k, std::min(k + csize, i1 + d)});
-            rl.count = (int)P.r0_jobs.size() - rl.first;
+                        for (int k = i1; k < i1 + d; k += csize) {
+                            const int kb = std::min(k + csize, i1 + d);
+                            if (!large) {
+                                P.r0_jobs.push_back(R0Job{p, i1, k, kb});
+                            } else {
+                                // heavier blocks (more k' blocks) first
+                                for (int D = nbk - 1; D >= 0; --D)
+                                    for (int BI = 0; BI + D < nbk; ++BI)
+                                        P.r0l_jobs.push_back(R0JobL{p, i1, k, kb, (BI << 16) | (BI + D)});
+                            }
+                        }
+            rl.count = (large ? (int)P.r0l_jobs.size() : (int)P.r0_jobs.size()) - rl.first;
             P.r0_launches.push_back(rl);
         }
     }
-    // S1 of diagonal d+1 is computed by the finalize launch of diagonal d (same Np class)
+    // S1 of diagonal d+1 is computed by the finalize launch of diagonal d (same class)
     for (auto &fl : P.fin_launches)
         for (const auto &nx : P.fin_launches)
-            if (nx.d == fl.d + 1 && nx.nb == fl.nb) { fl.s1_first = nx.first; fl.s1_count = nx.count; }
+            if (nx.d == fl.d + 1 && nx.np == fl.np) { fl.s1_first = nx.first; fl.s1_count = nx.count; }
     return BPMAX_OK;
+}
+
+void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L)
+{
+    const int grid = std::min(L.count, 3 * ctx->sms);
+    r0_large_kernel<<<grid, 128, R0Shape<8>::SMEM, ctx->stream>>>(
+        (const R0JobL *)ctx->r0ljobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
+        (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
+}
+
+void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L)
+{
+    constexpr int W = FIN_LARGE_THREADS / 32;
+    finalize_large_kernel<<<L.count + (L.s1_count + W - 1) / W, FIN_LARGE_THREADS, 0, ctx->stream>>>(
+        (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
+        (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
+        (const uint8_t *)ctx->bases.p, ctx->W, L.d);
 }
 
 template <int NB>
@@ -189,7 +233,7 @@ void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L)
 template <int NB>
 void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L)
 {
-    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, 0, ctx->stream>>>(
+    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, FinShape<8 * NB>::SMEM, ctx->stream>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
         (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
         (const uint8_t *)ctx->bases.p, ctx->W, L.d);
@@ -199,6 +243,10 @@ template <int NB>
 int set_smem_attr(bpmax_ctx *ctx)
 {
     CK(cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<NB>::SMEM));
+    CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)FinShape<8 * NB>::SMEM));
+    if (NB == 8)
+        CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<8>::SMEM));
     return BPMAX_OK;
 }
 
@@ -240,14 +288,16 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         ProfScope ps(ctx, kp, 0);
         single_strand_kernel<<<(int)P.pairs.size(), 512, 0, ctx->stream>>>(
             (const PairDesc *)ctx->pairs.p, (const uint8_t *)ctx->bases.p, (float *)ctx->S.p, ctx->W);
+        s2_aux_kernel<<<(int)P.pairs.size(), 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (float *)ctx->S.p);
     }
-    ++launches;
+    launches += 2;
     size_t ri = 0, fi = 0;
     for (int d = 0; d < P.maxM; ++d) {
         for (; ri < P.r0_launches.size() && P.r0_launches[ri].d == d; ++ri, ++launches) {
             const auto &L = P.r0_launches[ri];
             ProfScope ps(ctx, kp, 1);
-            switch (L.nb) {
+            switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
+            case 0: launch_r0_large(ctx, L); break;
             case 1: launch_r0<1>(ctx, L); break;
             case 2: launch_r0<2>(ctx, L); break;
             case 3: launch_r0<3>(ctx, L); break;
@@ -261,7 +311,8 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         for (; fi < P.fin_launches.size() && P.fin_launches[fi].d == d; ++fi, ++launches) {
             const auto &L = P.fin_launches[fi];
             ProfScope ps(ctx, kp, 2);
-            switch (L.nb) {
+            switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
+            case 0: launch_fin_large(ctx, L); break;
             case 1: launch_fin<1>(ctx, L); break;
             case 2: launch_fin<2>(ctx, L); break;
             case 3: launch_fin<3>(ctx, L); break;
@@ -296,11 +347,15 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
         if ((st = ensure(ctx, ctx->bases, P.bases_bytes + 16)) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->pairs, P.pairs.size() * sizeof(PairDesc))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->r0jobs, P.r0_jobs.size() * sizeof(R0Job))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->r0ljobs, P.r0l_jobs.size() * sizeof(R0JobL))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->celljobs, P.cell_jobs.size() * sizeof(CellJob))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->scores, P.pairs.size() * sizeof(float))) != BPMAX_OK) return st;
         CK(cudaMemcpyAsync(ctx->pairs.p, P.pairs.data(), P.pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, ctx->stream));
         if (!P.r0_jobs.empty())
             CK(cudaMemcpyAsync(ctx->r0jobs.p, P.r0_jobs.data(), P.r0_jobs.size() * sizeof(R0Job), cudaMemcpyHostToDevice, ctx->stream));
+        if (!P.r0l_jobs.empty())
+            CK(cudaMemcpyAsync(ctx->r0ljobs.p, P.r0l_jobs.data(), P.r0l_jobs.size() * sizeof(R0JobL), cudaMemcpyHostToDevice,
+                               ctx->stream));
         CK(cudaMemcpyAsync(ctx->celljobs.p, P.cell_jobs.data(), P.cell_jobs.size() * sizeof(CellJob), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->plan_valid = true;
@@ -354,7 +409,7 @@ int check_pair(bpmax_ctx *ctx, const int *s1, long M, const int *s2, long N)
 {
     if (!s1 || !s2) return fail(ctx, BPMAX_EINVAL, "null sequence pointer");
     if (M < 1 || N < 1) return fail(ctx, BPMAX_EINVAL, "sequence lengths must be >= 1 (M=%ld, N=%ld)", M, N);
-    if (M > 65535 || N > 65535) return fail(ctx, BPMAX_EINVAL, "sequence length too large");
+    if (M > 65535 || N > MAX_NP) return fail(ctx, BPMAX_EINVAL, "sequence length too large (M=%ld, N=%ld)", M, N);
     for (long i = 0; i < M; ++i)
         if (s1[i] < 0 || s1[i] > 4) return fail(ctx, BPMAX_EINVAL, "seq1[%ld]=%d is not a base code 0..4", i, s1[i]);
     for (long i = 0; i < N; ++i)
@@ -471,7 +526,7 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
-    for (DevBuf *b : {&ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs, &ctx->r0jobs, &ctx->celljobs,
+    for (DevBuf *b : {&ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs, &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs,
                       &ctx->scores, &ctx->conv})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
@@ -726,8 +781,11 @@ __global__ void noalloc_r0_jobs_kernel(R0Job *__restrict__ jobs, int cells, int 
 template <int NB>
 int noalloc_set_attr()
 {
-    return cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)R0Shape<NB>::SMEM) == cudaSuccess ? BPMAX_OK : BPMAX_ECUDA;
+    if (cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<NB>::SMEM) !=
+        cudaSuccess)
+        return BPMAX_ECUDA;
+    return cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)FinShape<8 * NB>::SMEM) == cudaSuccess ? BPMAX_OK : BPMAX_ECUDA;
 }
 
 // Once per device, with that device current: the device address of the scratch array (a host
@@ -768,8 +826,8 @@ void noalloc_launch_diag(cudaStream_t s, int sms, int d, int n_r0, int n_cells, 
         r0_small_kernel<NB><<<std::min(n_r0, 3 * sms), R0Shape<NB>::THREADS, R0Shape<NB>::SMEM, s>>>(rj, n_r0, pd, F,
                                                                                                  FT, S, d);
     const int n_s1 = n_cells - 1;  // S1 cells of diagonal d+1: the first n_cells-1 entries of cj
-    finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + 3) / 4, 128, 0, s>>>(cj, n_cells, cj, n_s1, pd, F, FT, S, bases,
-                                                                          W, d);
+    finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + 3) / 4, 128, FinShape<8 * NB>::SMEM, s>>>(
+        cj, n_cells, cj, n_s1, pd, F, FT, S, bases, W, d);
 }
 
 }  // namespace

@@ -33,6 +33,8 @@ struct PairDesc {
     long long F_off;   // float offset of F[0] (and of FT[0] in the FT arena)
     long long S1_off;  // float offset of S1 in the S arena
     long long S2_off;  // float offset of S2 in the S arena
+    long long S2m_off; // Np > 64 only: S2 with -inf outside its triangle
+    long long S2t_off; // Np > 64 only: ST1[j][k] = S2(k+1, j), -inf outside
     int seq1_off;      // offset of seq1 in the base arena (uint8)
     int seq2_off;      // offset of the REVERSED seq2 in the base arena (uint8)
 };
@@ -363,15 +365,28 @@ struct CellJob {
 };
 
 template <int NP>
+struct FinShape {
+    static constexpr int LD = NP + 4;             // 16-byte rows; conflict-free column walks
+    static constexpr int TBL = NP * LD;           // one NP x NP table
+    static constexpr size_t SMEM = 4 * (size_t)TBL * sizeof(float) + NP;
+};
+
+// The inner DP reads, for cell (i2,j2):  R1 = max_k F[i2][k] + S2[k+1][j2],  R2 = max_k S2[i2][k] + F[k+1][j2].
+// Shared memory keeps F and S2 row-major plus shifted transposes FT1[j2][k] = F[k+1][j2] and
+// ST1[j2][k] = S2[k+1][j2], so both are row-by-row scans with 16-byte loads. Every entry outside
+// the logical triangles is -inf, so 4-aligned k chunks that overhang [i2, j2) only add -inf terms
+// (k < i2 meets F[i2][k] or S2[i2][k]; k >= j2 meets ST1[j2][k] or FT1[j2][k]).
+template <int NP>
 __global__ void __launch_bounds__(128)
 finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
                       const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
                       float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
 {
-    constexpr int LD = NP + 4;  // 16-byte rows; odd multiple of 4 words per row keeps column walks conflict-free
-    __shared__ __align__(16) float Fs[NP * LD];
-    __shared__ __align__(16) float Ss[NP * LD];
-    __shared__ uint8_t sb[NP];
+    using Sh = FinShape<NP>;
+    constexpr int LD = Sh::LD;
+    extern __shared__ __align__(16) float fsm[];
+    float *Fs = fsm, *FT1 = fsm + Sh::TBL, *Ss = fsm + 2 * Sh::TBL, *ST1 = fsm + 3 * Sh::TBL;
+    uint8_t *sb = reinterpret_cast<uint8_t *>(fsm + 4 * Sh::TBL);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if ((int)blockIdx.x >= njobs) {  // S1 cells (i, i+d+1), one per warp
         const int q = ((int)blockIdx.x - njobs) * 4 + warp;
@@ -404,54 +419,59 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     const float *S2 = S + pd.S2_off;
     const uint8_t *s1 = bases + pd.seq1_off;
     const uint8_t *s2r = bases + pd.seq2_off;
-    constexpr int CPR = NP / 4;
-    for (int q = tid; q < 2 * NP * CPR; q += 128) {
-        const int which = q / (NP * CPR), r = (q / CPR) % NP, c = (q % CPR) * 4;
-        if (which == 0) cp_async16(Fs + r * LD + c, Fc + r * NP + c);
-        else cp_async16(Ss + r * LD + c, S2 + r * NP + c);
-    }
-    cp_async_commit();
-    for (int q = tid; q < NP; q += 128) sb[q] = q < N ? s2r[q] : 4;
     const float s1v = S1[i1 * M + j1];
-    cp_async_wait<0>();
-    __syncthreads();
-    // init candidates
-    for (int q = tid; q < NP * NP; q += 128) {
-        const int r = q / NP, c = q % NP;
-        float v = NEG_INF;
-        if (r <= c && c < N) {
-            if (d == 0 && r == c) v = score_w(W.w + 6, s1[i1], sb[r]);
-            else v = fmaxf(Fs[r * LD + c], s1v + Ss[r * LD + c]);
+    for (int q = tid; q < NP; q += 128) sb[q] = q < N ? s2r[q] : 4;
+    __syncthreads();  // sb is read by the staging loop (inter-strand base case)
+    // staging: 16-byte loads of the accumulated F (max of R0, R3, R4, SW1) and of S2
+    for (int q4 = tid; q4 < NP * NP / 4; q4 += 128) {
+        const int r = (4 * q4) / NP, c0 = (4 * q4) % NP;
+        const float4 a = *reinterpret_cast<const float4 *>(Fc + 4 * q4);
+        const float4 b = *reinterpret_cast<const float4 *>(S2 + 4 * q4);
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+        float fv[4], sv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int c = c0 + e;
+            const bool valid = r <= c && c < N;
+            sv[e] = valid ? bv[e] : NEG_INF;
+            float v = NEG_INF;
+            if (valid) v = (d == 0 && r == c) ? score_w(W.w + 6, s1[i1], sb[r]) : fmaxf(av[e], s1v + bv[e]);
+            fv[e] = v;
+            if (r >= 1) { FT1[c * LD + r - 1] = v; ST1[c * LD + r - 1] = sv[e]; }
         }
-        Fs[r * LD + c] = v;
+        *reinterpret_cast<float4 *>(Fs + r * LD + c0) = make_float4(fv[0], fv[1], fv[2], fv[3]);
+        *reinterpret_cast<float4 *>(Ss + r * LD + c0) = make_float4(sv[0], sv[1], sv[2], sv[3]);
     }
+    for (int c = tid; c < NP; c += 128) { FT1[c * LD + NP - 1] = NEG_INF; ST1[c * LD + NP - 1] = NEG_INF; }
     __syncthreads();
     for (int dd = 1; dd < N; ++dd) {
-        const int cells = N - dd;
-        int g = 1;
-        while (g < 32 && g * 2 * cells <= 128) g *= 2;
+        const int cells = N - dd;  // <= 63 < 128: one pass
+        const int g = min(32, 1 << (31 - __clz(128 / cells)));
         const int lane_g = tid & (g - 1);
-        const int slots = 128 / g;
-        for (int base = 0; base < cells; base += slots) {
-            const int i2 = base + tid / g, j2 = i2 + dd;
-            const bool act = i2 < cells;
-            float r0 = NEG_INF, r1 = NEG_INF;
-            if (act) {
-                int k = i2 + lane_g;
-                for (; k + g < j2; k += 2 * g) {
-                    r0 = fmax3(r0, Fs[i2 * LD + k] + Ss[(k + 1) * LD + j2], Ss[i2 * LD + k] + Fs[(k + 1) * LD + j2]);
-                    r1 = fmax3(r1, Fs[i2 * LD + k + g] + Ss[(k + g + 1) * LD + j2],
-                               Ss[i2 * LD + k + g] + Fs[(k + g + 1) * LD + j2]);
-                }
-                if (k < j2) r0 = fmax3(r0, Fs[i2 * LD + k] + Ss[(k + 1) * LD + j2], Ss[i2 * LD + k] + Fs[(k + 1) * LD + j2]);
+        const int i2 = tid / g, j2 = i2 + dd;
+        const bool act = i2 < cells;
+        float r0 = NEG_INF, r1 = NEG_INF;
+        if (act) {
+            const float *fr = Fs + i2 * LD, *sr = Ss + i2 * LD, *ftr = FT1 + j2 * LD, *str = ST1 + j2 * LD;
+            const int c_end = (j2 + 3) >> 2;
+            for (int c = (i2 >> 2) + lane_g; c < c_end; c += g) {
+                const float4 f = *reinterpret_cast<const float4 *>(fr + 4 * c);
+                const float4 t = *reinterpret_cast<const float4 *>(str + 4 * c);
+                const float4 s2 = *reinterpret_cast<const float4 *>(sr + 4 * c);
+                const float4 u = *reinterpret_cast<const float4 *>(ftr + 4 * c);
+                r0 = fmax3(r0, f.x + t.x, s2.x + u.x);
+                r1 = fmax3(r1, f.y + t.y, s2.y + u.y);
+                r0 = fmax3(r0, f.z + t.z, s2.z + u.z);
+                r1 = fmax3(r1, f.w + t.w, s2.w + u.w);
             }
-            float red = fmaxf(r0, r1);
-            for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
-            if (act && lane_g == 0) {
-                float v = fmaxf(Fs[i2 * LD + j2], red);
-                if (dd >= 4) v = fmaxf(v, Fs[(i2 + 1) * LD + (j2 - 1)] + score_w(W.w, sb[i2], sb[j2]));
-                Fs[i2 * LD + j2] = v;
-            }
+        }
+        float red = fmaxf(r0, r1);
+        for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
+        if (act && lane_g == 0) {
+            float v = fmaxf(Fs[i2 * LD + j2], red);
+            if (dd >= 4) v = fmaxf(v, Fs[(i2 + 1) * LD + (j2 - 1)] + score_w(W.w, sb[i2], sb[j2]));
+            Fs[i2 * LD + j2] = v;
+            if (i2 >= 1) FT1[j2 * LD + i2 - 1] = v;
         }
         __syncthreads();
     }
@@ -461,7 +481,7 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * tile : nullptr;
     for (int q4 = tid; q4 < NP * NP / 4; q4 += 128) {
         const int r = (4 * q4) / NP, c = (4 * q4) % NP;
-        const float4 v = *reinterpret_cast<const float4 *>(Fs + r * LD + c);
+        float4 v = *reinterpret_cast<const float4 *>(Fs + r * LD + c);
         if (push) {
             float4 u;
             u.x = (r <= c + 0 && c + 0 < N) ? v.x + wp : 0.0f;
@@ -470,16 +490,17 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
             u.w = (r <= c + 3 && c + 3 < N) ? v.w + wp : 0.0f;
             *reinterpret_cast<float4 *>(Fn + 4 * q4) = u;
         }
-    }
-    __syncthreads();
-    // S1(i1,j1) on the subdiagonal: the R3/R4 slots of the product kernel (never a logical cell)
-    for (int r = 1 + tid; r < NP; r += 128) Fs[r * LD + r - 1] = s1v;
-    __syncthreads();
-    for (int q4 = tid; q4 < NP * NP / 4; q4 += 128) {
-        const int r = (4 * q4) / NP, c = (4 * q4) % NP;
-        *reinterpret_cast<float4 *>(Fc + 4 * q4) = *reinterpret_cast<const float4 *>(Fs + r * LD + c);
-        *reinterpret_cast<float4 *>(FTc + 4 * q4) =
-            make_float4(Fs[c * LD + r], Fs[(c + 1) * LD + r], Fs[(c + 2) * LD + r], Fs[(c + 3) * LD + r]);
+        // S1(i1,j1) on the subdiagonal: the R3/R4 slots of the product kernel (never a logical cell)
+        if (r == c + 1) v.x = s1v;
+        if (r == c + 2) v.y = s1v;
+        if (r == c + 3) v.z = s1v;
+        if (r == c + 4) v.w = s1v;
+        *reinterpret_cast<float4 *>(Fc + 4 * q4) = v;
+        const float c0v = (r + 1 == c + 0) ? s1v : Fs[(c + 0) * LD + r];
+        const float c1v = (r + 1 == c + 1) ? s1v : Fs[(c + 1) * LD + r];
+        const float c2v = (r + 1 == c + 2) ? s1v : Fs[(c + 2) * LD + r];
+        const float c3v = (r + 1 == c + 3) ? s1v : Fs[(c + 3) * LD + r];
+        *reinterpret_cast<float4 *>(FTc + 4 * q4) = make_float4(c0v, c1v, c2v, c3v);
     }
 }
 

@@ -1,0 +1,309 @@
+// bpmax_kernels_large.cuh -- kernels for inner tables wider than 64 (Np = N rounded up to a
+// multiple of 64). Same recurrence, layout and exactness argument as bpmax_kernels.cuh.
+#pragma once
+#include "bpmax_kernels.cuh"
+
+namespace bpmax {
+
+// ------------------------------------------------------------------------------------------
+// Masked copies of S2 for the large finalize: S2M[i][k] = S2(i,k) if i <= k < N else -inf and
+// ST1[j][k] = S2(k+1,j) if k+1 <= j < N else -inf (S2 over the reversed strand 2,
+// V3/bpmax_verify.c:560-571). One CTA per pair; pairs with Np <= 64 are skipped.
+// ------------------------------------------------------------------------------------------
+__global__ void s2_aux_kernel(const PairDesc *__restrict__ pairs, float *__restrict__ S)
+{
+    const PairDesc pd = pairs[blockIdx.x];
+    if (pd.Np <= 64) return;
+    const int Np = pd.Np, N = pd.N;
+    const float *S2 = S + pd.S2_off;
+    float *S2M = S + pd.S2m_off, *ST1 = S + pd.S2t_off;
+    for (int q = threadIdx.x; q < Np * Np; q += blockDim.x) {
+        const int r = q / Np, c = q % Np;
+        S2M[q] = (r <= c && c < N) ? S2[q] : NEG_INF;
+        ST1[q] = (c + 1 <= r && r < N) ? S2[(c + 1) * Np + r] : NEG_INF;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// R0 + R3 + R4 (same triangular (max,+) product as r0_small_kernel: A_s = F(i1,k1) shifted one
+// column right with S1(i1,k1) on its diagonal, B = F(k1+1,j1) with S1(k1+1,j1) on its
+// subdiagonal) for Np = 64*NBk. A job is one outer cell, one 64x64 output block (BI,BJ) and a k1
+// range; it loops over the k' blocks KB in [BI, BJ]. Each stage holds rows k' = 64KB..64KB+64 of
+// A_s (columns i2 of block BI) and of B (columns j2 of block BJ) in the swizzled 64-wide layout
+// of r0_small_kernel<8>. Diagonal output blocks use its balanced triangular task table; the
+// other blocks give every thread one 8x8 micro-tile and half of the eight 8-wide k' sub-blocks
+// (A is triangular in the stage KB == BI, B in the stage KB == BJ, dense in between).
+// ------------------------------------------------------------------------------------------
+struct R0JobL {
+    int pair, i1, k1a, k1b, blk;  // blk = BI << 16 | BJ
+};
+
+__global__ void __launch_bounds__(128, 3)
+r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs, float *__restrict__ F,
+                const float *__restrict__ FT, const float *__restrict__ S, int d)
+{
+    using Sh = R0Shape<8>;
+    constexpr int B = 64;
+    extern __shared__ __align__(16) float smem[];
+    const int tid = threadIdx.x;
+    int jid = blockIdx.x;
+    if (jid >= njobs) return;
+
+    // issue the copies of (job, k1, KB) into stage
+    auto load_item = [&](int stage, const R0JobL &jb, int k1, int KB) {
+        const PairDesc pd = pairs[jb.pair];
+        const int M = pd.M, Np = pd.Np, NBk = Np / B, j1 = jb.i1 + d;
+        const int BI = jb.blk >> 16, BJ = jb.blk & 0xffff;
+        const long long tile = (long long)Np * Np;
+        float *st = smem + stage * Sh::STAGE;
+        const float *ga = FT + pd.F_off + cell_index(M, jb.i1, k1) * tile;
+        const float *gb = F + pd.F_off + cell_index(M, k1 + 1, j1) * tile;
+        const float *S1 = S + pd.S1_off;
+        for (int q = tid; q < 2 * (B + 1) * 16; q += 128) {
+            const int which = q / ((B + 1) * 16), r = (q / 16) % (B + 1), cc = q % 16;
+            const int kp = B * KB + r;  // global k'
+            if (which == 0) {
+                if (kp == 0) {  // A_s row 0: S1(i1,k1) at (0,0), -inf elsewhere
+                    float4 v = make_float4(NEG_INF, NEG_INF, NEG_INF, NEG_INF);
+                    if (BI == 0 && cc == 0) v.x = S1[jb.i1 * M + k1];
+                    *reinterpret_cast<float4 *>(st + r0_off<8>(r, 4 * cc)) = v;
+                } else {
+                    cp_async16(st + r0_off<8>(r, 4 * cc), ga + (long long)(kp - 1) * Np + B * BI + 4 * cc);
+                }
+            } else {
+                if (kp == Np) {  // guard row: S1(k1+1,j1) at (Np, Np-1), -inf elsewhere
+                    float4 v = make_float4(NEG_INF, NEG_INF, NEG_INF, NEG_INF);
+                    if (BJ == NBk - 1 && cc == 15) v.w = S1[(k1 + 1) * M + j1];
+                    *reinterpret_cast<float4 *>(st + Sh::A_FLOATS + r0_off<8>(r, 4 * cc)) = v;
+                } else {
+                    cp_async16(st + Sh::A_FLOATS + r0_off<8>(r, 4 * cc), gb + (long long)kp * Np + B * BJ + 4 * cc);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+
+    R0JobL job = jobs[jid];
+    int BI = job.blk >> 16, BJ = job.blk & 0xffff;
+    int k1 = job.k1a, KB = BI, stage = 0;
+    // per-job thread mapping (diagonal vs off-diagonal output block)
+    int bi = 0, bj = 0, kb = 0, h = 0;
+    bool has_task = false;
+    auto map_threads = [&]() {
+        if (BI == BJ) {
+            has_task = tid < R0Shape<8>::TASKS;
+            if (has_task) { bi = c_r0_lane64[tid][0]; bj = c_r0_lane64[tid][1]; kb = c_r0_lane64[tid][2]; }
+        } else {
+            has_task = true;
+            const int m = tid & 63;
+            bi = m >> 3;
+            bj = m & 7;
+            h = tid >> 6;
+        }
+    };
+    map_threads();
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = NEG_INF;
+
+    auto step8 = [&](const float *As, const float *Bs, int kbl) {
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+            const int r = 8 * kbl + k;
+            const float4 a0 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi));
+            const float4 a1 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi + 4));
+            const float4 a2 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r + 1, 8 * bi));
+            const float4 a3 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r + 1, 8 * bi + 4));
+            const float4 b0 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r, 8 * bj));
+            const float4 b1 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r, 8 * bj + 4));
+            const float4 b2 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r + 1, 8 * bj));
+            const float4 b3 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r + 1, 8 * bj + 4));
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float aw[8] = {a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const float bw[8] = {b2.x, b2.y, b2.z, b2.w, b3.x, b3.y, b3.z, b3.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmax3(acc[i][j], av[i] + bv[j], aw[i] + bw[j]);
+        }
+    };
+    auto edge_step = [&](const float *As, const float *Bs) {  // k' = 8bj+8 (local): R4 of column 8bj+7
+        const int r = 8 * bj + 8;
+        const float4 a0 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi));
+        const float4 a1 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi + 4));
+        const float bs = Bs[r0_off<8>(r, 8 * bj + 4) + 3];
+        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i][7] = fmaxf(acc[i][7], av[i] + bs);
+    };
+
+    load_item(0, job, k1, KB);
+    while (true) {
+        // next item: KB advances fastest, then k1, then the job
+        R0JobL njob = job;
+        int njid = jid, nk1 = k1, nKB = KB + 1;
+        if (nKB > BJ) {
+            nKB = -1;
+            nk1 = k1 + 1;
+            if (nk1 >= job.k1b) {
+                njid = jid + gridDim.x;
+                if (njid < njobs) { njob = jobs[njid]; nk1 = njob.k1a; }
+            }
+        }
+        const bool has_next = njid < njobs;
+        if (nKB < 0) nKB = has_next ? (njob.blk >> 16) : 0;
+        cp_async_wait<0>();
+        __syncthreads();
+        if (has_next) load_item(stage ^ 1, njob, nk1, nKB);
+        const float *As = smem + stage * Sh::STAGE;
+        const float *Bs = As + Sh::A_FLOATS;
+        if (has_task) {
+            if (BI == BJ) {
+                step8(As, Bs, kb);
+                if (kb == bj) edge_step(As, Bs);
+            } else {
+                int lo = 4 * h, hi = 4 * h + 4;
+                if (KB == BI) lo = max(lo, bi);
+                if (KB == BJ) hi = min(hi, bj + 1);
+                for (int kbl = lo; kbl < hi; ++kbl) step8(As, Bs, kbl);
+                if (KB == BJ && bj >= 4 * h && bj < 4 * h + 4) edge_step(As, Bs);
+            }
+        }
+        if (njid != jid || !has_next) {  // job done: merge its partial maxima into F(i1, i1+d)
+            if (has_task) {
+                const PairDesc pd = pairs[job.pair];
+                const long long tile = (long long)pd.Np * pd.Np;
+                int *out = reinterpret_cast<int *>(F + pd.F_off + cell_index(pd.M, job.i1, job.i1 + d) * tile);
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int i2 = B * BI + 8 * bi + i, j2 = B * BJ + 8 * bj + j;
+                        if (i2 <= j2 && j2 < pd.N) atomicMax(out + (long long)i2 * pd.Np + j2, __float_as_int(acc[i][j]));
+                        acc[i][j] = NEG_INF;
+                    }
+            }
+        }
+        if (!has_next) break;
+        if (njid != jid) {
+            job = njob;
+            BI = job.blk >> 16;
+            BJ = job.blk & 0xffff;
+            map_threads();
+        }
+        jid = njid;
+        k1 = nk1;
+        KB = nKB;
+        stage ^= 1;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Finalize for Np > 64: one CTA per outer cell of diagonal d, inner wavefront over the cell's
+// tables in global memory (L2-resident). Same candidates as finalize_small_kernel:
+//   base inter, S1+S2, SW1 (already in F, pushed two diagonals earlier), SW2, R1, R2;
+// F and FT are kept consistent during the wavefront so R2 reads rows of FT.
+// CTAs after the first njobs compute S1 on diagonal d+1, one warp per cell.
+// ------------------------------------------------------------------------------------------
+constexpr int FIN_LARGE_THREADS = 512;
+
+__global__ void __launch_bounds__(FIN_LARGE_THREADS)
+finalize_large_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
+                      const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
+                      float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
+{
+    constexpr int NT = FIN_LARGE_THREADS, WARPS = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if ((int)blockIdx.x >= njobs) {  // S1 cells (i, i+d+1), one per warp
+        const int q = ((int)blockIdx.x - njobs) * WARPS + warp;
+        if (q >= ns1) return;
+        const CellJob job = s1jobs[q];
+        const PairDesc pd = pairs[job.pair];
+        const int M = pd.M, i = job.i1, j = i + d + 1;
+        float *S1 = S + pd.S1_off;
+        if (j - i <= 3) return;
+        const uint8_t *s1 = bases + pd.seq1_off;
+        float red = NEG_INF;
+        for (int k = i + lane; k < j; k += 32) red = fmaxf(red, S1[i * M + k] + S1[(k + 1) * M + j]);
+        for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
+        if (lane == 0) S1[i * M + j] = fmaxf(S1[(i + 1) * M + (j - 1)] + score_w(W.w, s1[i], s1[j]), red);
+        return;
+    }
+    const CellJob job = jobs[blockIdx.x];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1, j1 = i1 + d;
+    const long long tile = (long long)Np * Np;
+    float *Fc = F + pd.F_off + cell_index(M, i1, j1) * tile;
+    float *FTc = FT + pd.F_off + cell_index(M, i1, j1) * tile;
+    const float *S1 = S + pd.S1_off;
+    const float *S2 = S + pd.S2_off;
+    const float *S2M = S + pd.S2m_off;
+    const float *ST1 = S + pd.S2t_off;
+    const uint8_t *s1 = bases + pd.seq1_off;
+    const uint8_t *s2r = bases + pd.seq2_off;
+    const float s1v = S1[i1 * M + j1];
+    for (long long q = tid; q < tile; q += NT) {
+        const int r = (int)(q / Np), c = (int)(q % Np);
+        float v = NEG_INF;
+        if (r <= c && c < N) v = (d == 0 && r == c) ? score_w(W.w + 6, s1[i1], s2r[r]) : fmaxf(Fc[q], s1v + S2[q]);
+        Fc[q] = v;
+    }
+    __syncthreads();
+    for (long long q = tid; q < tile; q += NT) {
+        const int r = (int)(q / Np), c = (int)(q % Np);
+        FTc[q] = Fc[(long long)c * Np + r];
+    }
+    __syncthreads();
+    for (int dd = 1; dd < N; ++dd) {
+        const int cells = N - dd;
+        int g = 1;
+        while (g < 32 && g * 2 * cells <= NT) g *= 2;
+        const int lane_g = tid & (g - 1);
+        const int slots = NT / g;
+        for (int base = 0; base < cells; base += slots) {
+            const int i2 = base + tid / g, j2 = i2 + dd;
+            const bool act = i2 < cells;
+            float r0 = NEG_INF, r1 = NEG_INF;
+            if (act) {
+                const float *fr = Fc + (long long)i2 * Np, *sr = S2M + (long long)i2 * Np;
+                const float *str = ST1 + (long long)j2 * Np, *ftr = FTc + (long long)j2 * Np + 1;
+                int k = i2 + lane_g;
+                for (; k + g < j2; k += 2 * g) {
+                    r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
+                    r1 = fmax3(r1, fr[k + g] + str[k + g], sr[k + g] + ftr[k + g]);
+                }
+                if (k < j2) r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
+            }
+            float red = fmaxf(r0, r1);
+            for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
+            if (act && lane_g == 0) {
+                float v = fmaxf(Fc[(long long)i2 * Np + j2], red);
+                if (dd >= 4)
+                    v = fmaxf(v, Fc[(long long)(i2 + 1) * Np + (j2 - 1)] + score_w(W.w, s2r[i2], s2r[j2]));
+                Fc[(long long)i2 * Np + j2] = v;
+                FTc[(long long)j2 * Np + i2] = v;
+            }
+        }
+        __syncthreads();
+    }
+    // SW1 candidate of cell (i1-1, j1+1), whose table nothing else has written yet
+    if (i1 >= 1 && j1 + 1 < M && d + 2 >= 4) {
+        const float wp = score_w(W.w, s1[i1 - 1], s1[j1 + 1]);
+        float *Fn = F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * tile;
+        for (long long q = tid; q < tile; q += NT) {
+            const int r = (int)(q / Np), c = (int)(q % Np);
+            Fn[q] = (r <= c && c < N) ? Fc[q] + wp : 0.0f;
+        }
+    }
+    __syncthreads();
+    // S1(i1,j1) on the subdiagonal of F (and the superdiagonal of FT): the R3/R4 slots
+    for (int r = 1 + tid; r < Np; r += NT) {
+        Fc[(long long)r * Np + r - 1] = s1v;
+        FTc[(long long)(r - 1) * Np + r] = s1v;
+    }
+}
+
+}  // namespace bpmax

@@ -128,3 +128,37 @@ def test_dropin_shim_links_like_reference_wrapper(tmp_path, oracle_mod):
     mine = oracle_mod.to_reference_layout(Fo, M, N, T)
     assert np.array_equal(bits(mine[mask]), bits(Fr[mask]))
     assert f"F(0,{M - 1},0,{N - 1})" in r.stdout
+
+
+@pytest.mark.parametrize("M,N,seed,wkind", [
+    (5, 65, 51, "int"), (7, 100, 52, "real"), (12, 130, 53, "int"), (3, 256, 54, "int"), (9, 200, 55, "real"),
+    (16, 128, 56, "int"),
+])
+def test_wide_inner_tables_vs_oracle(eng, oracle_mod, M, N, seed, wkind):
+    """Strand-2 lengths above 64 take the blocked product and the global-memory inner wavefront."""
+    s1, s2 = W.pair(M, N, seed)
+    w = W.INTEGER_WEIGHTS if wkind == "int" else W.random_weights(seed)
+    eng.set_weights(w)
+    F, score = eng.fill_compact(s1, s2)
+    Fo, _, _ = oracle_mod.fill(s1, s2, w)
+    assert np.array_equal(bits(F), bits(Fo))
+    assert score == oracle_mod.score(Fo, M, N)
+
+
+def test_wide_inner_reference_layout(eng, oracle_mod):
+    M, N, T = 6, 150, 64
+    s1, s2 = W.pair(M, N, 57)
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    Fr, _ = eng.fill(s1, s2, T)
+    Fo, _, _ = oracle_mod.fill(s1, s2, W.INTEGER_WEIGHTS)
+    mask = oracle_mod.reference_written_mask(M, N, T)
+    assert np.array_equal(bits(oracle_mod.to_reference_layout(Fo, M, N, T)[mask]), bits(Fr[mask]))
+
+
+def test_batched_mixed_widths(eng, oracle_mod):
+    pairs = [W.pair(m, n, 60 + i) for i, (m, n) in enumerate([(9, 70), (14, 20), (5, 130), (11, 64), (8, 8), (3, 90)])]
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    got = eng.score_batch(pairs)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
+                   dtype=np.float32)
+    assert np.array_equal(bits(got), bits(exp))
