@@ -23,6 +23,7 @@
 #include "../../include/bpmax_gpu.h"
 #include "bpmax_kernels.cuh"
 #include "bpmax_kernels_large.cuh"
+#include "bpmax_adjoint.cuh"
 
 using namespace bpmax;
 
@@ -64,7 +65,7 @@ struct bpmax_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
     std::string err;
-    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv;
+    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus;
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -526,7 +527,7 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
-    for (DevBuf *b : {&ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs, &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs,
+    for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs, &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs,
                       &ctx->scores, &ctx->conv})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
@@ -663,10 +664,36 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
     return BPMAX_OK;
 }
 
-int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int, const int *const *, const long *, const int *const *, const long *,
-                         float *, float *)
+int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                         const int *const *seq2s, const long *Ns, float *scores, float *grads)
 {
-    return fail(ctx, BPMAX_EINVAL, "gradients are not available in this build");
+    if (!ctx) return BPMAX_EINVAL;
+    int st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
+    if (st) return st;
+    long maxlen = 0;
+    for (int p = 0; p < num_pairs; ++p) maxlen = std::max(maxlen, Ms[p] + Ns[p]);
+    const int cap = (int)(2 * maxlen + 64);  // DFS depth of the argmax tree <= M + N + 1
+    if ((st = ensure(ctx, ctx->tbstack, (size_t)num_pairs * cap * sizeof(TbNode))) != BPMAX_OK) return st;
+    if ((st = ensure(ctx, ctx->grads, (size_t)num_pairs * 12 * sizeof(float))) != BPMAX_OK) return st;
+    if ((st = ensure(ctx, ctx->tbstatus, (size_t)num_pairs * sizeof(int))) != BPMAX_OK) return st;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    traceback_kernel<<<num_pairs, TB_THREADS, 0, ctx->stream>>>(
+        (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (const float *)ctx->S.p, (const uint8_t *)ctx->bases.p,
+        ctx->W, (TbNode *)ctx->tbstack.p, cap, (float *)ctx->grads.p, (int *)ctx->tbstatus.p);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    std::vector<int> stat(num_pairs);
+    CK(cudaMemcpyAsync(stat.data(), ctx->tbstatus.p, num_pairs * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (scores) CK(cudaMemcpyAsync(scores, ctx->scores.p, num_pairs * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    if (grads) CK(cudaMemcpyAsync(grads, ctx->grads.p, num_pairs * 12 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    float tb_ms = 0.f;
+    CK(cudaEventElapsedTime(&tb_ms, ctx->ev0, ctx->ev1));
+    ctx->last_ms += tb_ms;
+    ctx->last_launches += 1;
+    for (int p = 0; p < num_pairs; ++p)
+        if (stat[p]) return fail(ctx, BPMAX_ECUDA, "adjoint pass of pair %d stopped (status %d)", p, stat[p]);
+    return BPMAX_OK;
 }
 
 int bpmax_gpu_profile_kernels(bpmax_ctx *ctx, float *ms, long *launches, double *terms)
