@@ -85,7 +85,8 @@ def _ptr(a: np.ndarray):
 
 def score_noalloc(seq1, seq2, w12, stream: int | None = None) -> float:
     """bpmax_gpu_score_noalloc: one pair's score with no memory allocated by the library (its
-    scratch is a fixed 64 MiB device array). Raises BpmaxError on a non-zero status."""
+    scratch is a fixed 64 MiB device array, enough for N <= 64 and M <= 114 at N = 64).
+    Raises BpmaxError on a non-zero status."""
     L = load_library()
     a, b = _seq(seq1), _seq(seq2)
     w = np.ascontiguousarray(np.asarray(w12, dtype=np.float32))

@@ -61,8 +61,6 @@ traceback_kernel(const PairDesc *__restrict__ pairs, const float *__restrict__ F
 {
     const PairDesc pd = pairs[blockIdx.x];
     const int M = pd.M, N = pd.N, Np = pd.Np;
-    const long long tile = (long long)Np * Np;
-    const float *Fp = F + pd.F_off;
     const float *S1 = S + pd.S1_off;
     const float *S2 = S + pd.S2_off;
     const uint8_t *s1 = bases + pd.seq1_off;
@@ -72,7 +70,7 @@ traceback_kernel(const PairDesc *__restrict__ pairs, const float *__restrict__ F
     __shared__ TbNode cur;
     __shared__ float cnt[12];
     __shared__ unsigned long long red[TB_THREADS / 32][5];
-    auto Fv = [&](int a, int b, int x, int y) { return Fp[cell_index(M, a, b) * tile + (long long)x * Np + y]; };
+    auto Fv = [&](int a, int b, int x, int y) { return f_value(pd, F, cell_index(M, a, b), x, y); };
     const int tid = threadIdx.x;
     if (tid < 12) cnt[tid] = 0.0f;
     if (tid == 0) {

@@ -4,8 +4,8 @@
 // Schedule of one fill (any number of pairs of uneven lengths, batched on one stream):
 //   clear F; single-strand tables S1, S2 of every pair;
 //   for d = 0 .. max(M)-1:                     (outer wavefront over j1-i1, V3/bpmax.c:300-323)
-//     R0+R3+R4 product kernel over the cells (i1, i1+d) of every pair with M > d, k1 split
-//       into chunks so that every diagonal launches enough CTAs to fill the GPU;
+//     R0+R3+R4 product kernel over the cells (i1, i1+d) of every pair with M > d: jobs of k1
+//       offset pairs (w, d-1-w), ordered by offset pair so both uses of a table meet in L2;
 //     finalize kernel over the same cells (init, SW1, inner R1/R2/SW2 wavefront, FT copy).
 // The whole sequence is captured once per shape as a CUDA graph and replayed.
 #include <cuda_runtime.h>
@@ -23,6 +23,7 @@
 #include "../../include/bpmax_gpu.h"
 #include "bpmax_kernels.cuh"
 #include "bpmax_kernels_large.cuh"
+#include "bpmax_r0.cuh"
 #include "bpmax_adjoint.cuh"
 
 using namespace bpmax;
@@ -44,6 +45,7 @@ struct Plan {
     std::vector<int> Ms, Ns;
     std::vector<PairDesc> pairs;
     long long F_floats = 0, S_floats = 0;
+    bool any_wide = false;  // some pair has Np > 64 (row-major tables + FT)
     int bases_bytes = 0;
     int maxM = 0;
     // per diagonal and Np class (index NB-1): ranges in the job arrays
@@ -65,7 +67,9 @@ struct bpmax_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
     std::string err;
-    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus;
+    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
+    int r0_occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class NB
+    int r0_pairs_per_job = 1 << 20;                 // upper bound of k1 offset pairs per product job
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -133,7 +137,8 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         pd.Np = padded_width(Ns[p]);
         if (pd.Np > MAX_NP) return fail(ctx, BPMAX_EINVAL, "strand-2 length %d > %d is not supported", Ns[p], MAX_NP);
         pd.F_off = f;
-        f = align64(f + (long long)Ms[p] * (Ms[p] + 1) / 2 * pd.Np * pd.Np);
+        f = align64(f + (long long)Ms[p] * (Ms[p] + 1) / 2 * cell_floats(pd.Np));
+        if (pd.Np > MAX_SMALL_NP) P.any_wide = true;
         pd.S1_off = s;
         s = align64(s + (long long)Ms[p] * Ms[p]);
         pd.S2_off = s;
@@ -159,7 +164,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     std::sort(classes.begin(), classes.end());
     classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
     // jobs, grouped by diagonal then inner width class
-    const int target = 4 * ctx->sms;  // CTAs per diagonal launch worth splitting k1 for
+    const int target = 4 * ctx->sms;  // CTAs per diagonal launch worth splitting k1 for (wide tables)
     for (int d = 0; d < P.maxM; ++d) {
         for (int np : classes) {
             long long cells = 0;
@@ -173,27 +178,42 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
             fl.count = (int)P.cell_jobs.size() - fl.first;
             P.fin_launches.push_back(fl);
             if (d == 0) continue;
-            const bool large = np > MAX_SMALL_NP;
+            if (np <= MAX_SMALL_NP) {
+                // jobs of q offset pairs (w, d-1-w), ordered by pair chunk, then pair, then cell: the
+                // two uses of a table (A of cell (a, a+d) at offset w, B of cell (a+w-d, a+w) at
+                // offset d-1-w) fall in the same pair chunk
+                const int NB = np / 8, G = R0_TAB_ITEMS[NB];
+                const long long P2 = (d + 1) / 2;  // offset pairs per cell
+                const long long resident = (long long)std::max(1, ctx->r0_occ[NB]) * ctx->sms;
+                // about two jobs per resident CTA: each job ends with one merge of the cell's tile
+                const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(ctx->r0_pairs_per_job, qmin);
+                const long long q = std::max(qmin, std::min(qmax, (cells * P2 + 2 * resident - 1) / (2 * resident)));
+                Plan::Launch rl{d, np, (int)P.r0_jobs.size(), 0};
+                for (long long c0 = 0; c0 < P2; c0 += q)
+                    for (int p = 0; p < n; ++p)
+                        if (P.pairs[p].Np == np && Ms[p] > d)
+                            for (int i1 = 0; i1 < Ms[p] - d; ++i1)
+                                P.r0_jobs.push_back(R0Job{p, i1, (int)c0, (int)std::min(c0 + q, P2)});
+                rl.count = (int)P.r0_jobs.size() - rl.first;
+                P.r0_launches.push_back(rl);
+                continue;
+            }
             const int nbk = np / 64;
-            const long long units = large ? cells * (nbk * (nbk + 1) / 2) : cells;
+            const long long units = cells * (nbk * (nbk + 1) / 2);
             long long chunks = std::max(1LL, std::min((long long)d, (target + units - 1) / units));
             int csize = (int)((d + chunks - 1) / chunks);
-            Plan::Launch rl{d, np, large ? (int)P.r0l_jobs.size() : (int)P.r0_jobs.size(), 0};
+            Plan::Launch rl{d, np, (int)P.r0l_jobs.size(), 0};
             for (int p = 0; p < n; ++p)
                 if (P.pairs[p].Np == np && Ms[p] > d)
                     for (int i1 = 0; i1 < Ms[p] - d; ++i1)
                         for (int k = i1; k < i1 + d; k += csize) {
                             const int kb = std::min(k + csize, i1 + d);
-                            if (!large) {
-                                P.r0_jobs.push_back(R0Job{p, i1, k, kb});
-                            } else {
-                                // heavier blocks (more k' blocks) first
-                                for (int D = nbk - 1; D >= 0; --D)
-                                    for (int BI = 0; BI + D < nbk; ++BI)
-                                        P.r0l_jobs.push_back(R0JobL{p, i1, k, kb, (BI << 16) | (BI + D)});
-                            }
+                            // heavier blocks (more k' blocks) first
+                            for (int D = nbk - 1; D >= 0; --D)
+                                for (int BI = 0; BI + D < nbk; ++BI)
+                                    P.r0l_jobs.push_back(R0JobL{p, i1, k, kb, (BI << 16) | (BI + D)});
                         }
-            rl.count = (large ? (int)P.r0l_jobs.size() : (int)P.r0_jobs.size()) - rl.first;
+            rl.count = (int)P.r0l_jobs.size() - rl.first;
             P.r0_launches.push_back(rl);
         }
     }
@@ -207,7 +227,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
 void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L)
 {
     const int grid = std::min(L.count, 3 * ctx->sms);
-    r0_large_kernel<<<grid, 128, R0Shape<8>::SMEM, ctx->stream>>>(
+    r0_large_kernel<<<grid, 128, WideShape::SMEM, ctx->stream>>>(
         (const R0JobL *)ctx->r0ljobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
         (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
 }
@@ -224,11 +244,11 @@ void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L)
 template <int NB>
 void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L)
 {
-    using Sh = R0Shape<NB>;
-    const int grid = std::min(L.count, 3 * ctx->sms);  // resident CTAs; each loops over jobs
-    r0_small_kernel<NB><<<grid, Sh::THREADS, Sh::SMEM, ctx->stream>>>(
-        (const R0Job *)ctx->r0jobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
-        (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
+    using C = R0Cfg<NB>;
+    const int grid = std::min(L.count, std::max(1, ctx->r0_occ[NB]) * ctx->sms);  // resident CTAs; each loops over jobs
+    r0_kernel<NB><<<grid, C::THREADS, C::SMEM, ctx->stream>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
+                                                              (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
+                                                              (int *)ctx->errflag.p);
 }
 
 template <int NB>
@@ -236,18 +256,19 @@ void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L)
 {
     finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, FinShape<8 * NB>::SMEM, ctx->stream>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
-        (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
-        (const uint8_t *)ctx->bases.p, ctx->W, L.d);
+        (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W,
+        L.d);
 }
 
 template <int NB>
 int set_smem_attr(bpmax_ctx *ctx)
 {
-    CK(cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<NB>::SMEM));
+    CK(cudaFuncSetAttribute(r0_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM));
     CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)FinShape<8 * NB>::SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ[NB], r0_kernel<NB>, R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM));
     if (NB == 8)
-        CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<8>::SMEM));
+        CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideShape::SMEM));
     return BPMAX_OK;
 }
 
@@ -285,6 +306,7 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
     long launches = 0;
     CK(cudaMemsetAsync(ctx->F.p, 0, (size_t)P.F_floats * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->S.p, 0, (size_t)P.S_floats * sizeof(float), ctx->stream));  // S1 starts at 0
+    CK(cudaMemsetAsync(ctx->errflag.p, 0, sizeof(int), ctx->stream));
     {
         ProfScope ps(ctx, kp, 0);
         single_strand_kernel<<<(int)P.pairs.size(), 512, 0, ctx->stream>>>(
@@ -343,7 +365,8 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
         if ((st = build_plan(ctx, Ms, Ns, ctx->plan)) != BPMAX_OK) return st;
         Plan &P = ctx->plan;
         if ((st = ensure(ctx, ctx->F, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
-        if ((st = ensure(ctx, ctx->FT, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
+        if (P.any_wide && (st = ensure(ctx, ctx->FT, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->errflag, sizeof(int))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->S, P.S_floats * sizeof(float))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->bases, P.bases_bytes + 16)) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->pairs, P.pairs.size() * sizeof(PairDesc))) != BPMAX_OK) return st;
@@ -400,9 +423,13 @@ int run_fill(bpmax_ctx *ctx)
     gather_scores_kernel<<<((int)P.pairs.size() + 127) / 128, 128, 0, ctx->stream>>>(
         (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)P.pairs.size(), (float *)ctx->scores.p);
     CK(cudaGetLastError());
+    int errv = 0;
+    CK(cudaMemcpyAsync(&errv, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
     ctx->last_launches = P.launches;
+    if (errv) return fail(ctx, BPMAX_ETIMEOUT, "a product kernel gave up waiting for its operand copies");
     return BPMAX_OK;
 }
 
@@ -527,8 +554,8 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
-    for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs, &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs,
-                      &ctx->scores, &ctx->conv})
+    for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs,
+                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs, &ctx->scores, &ctx->conv, &ctx->errflag})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
         if (ctx->host_stage[i]) cudaFreeHost(ctx->host_stage[i]);
@@ -601,11 +628,10 @@ int bpmax_gpu_fill_compact(bpmax_ctx *ctx, const int *seq1, long M, const int *s
     if (st) return st;
     if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
     if (!F_compact) return BPMAX_OK;
-    const PairDesc &pd = ctx->plan.pairs[0];
     const long long n_out = M * (M + 1) / 2 * N * N;
     if ((st = ensure(ctx, ctx->conv, n_out * sizeof(float))) != BPMAX_OK) return st;
-    to_compact_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>((const float *)ctx->F.p + pd.F_off, (int)M, (int)N,
-                                                             pd.Np, n_out, (float *)ctx->conv.p);
+    to_compact_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p,
+                                                             n_out, (float *)ctx->conv.p);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(F_compact, ctx->conv.p, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -624,7 +650,6 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
     if (st) return st;
     if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
     if (!F_lin) return BPMAX_OK;
-    const PairDesc &pd = ctx->plan.pairs[0];
     const long long cell_f = (long long)Ns * Ns * (N_tile + 1) * N_tile;
     // outer row i1 of the reference layout: cells (i1, i1..M-1) are contiguous
     const long long row_max = (long long)M * cell_f;
@@ -644,7 +669,7 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
             pending_dst[slot] = nullptr;
         }
         to_reference_row_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>(
-            (const float *)ctx->F.p + pd.F_off, (int)M, (int)N, pd.Np, (int)N_tile, (int)Ns, (int)i1, n_out, dbuf);
+            (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)N_tile, (int)Ns, (int)i1, n_out, dbuf);
         CK(cudaGetLastError());
         if (pinned) {
             CK(cudaMemcpyAsync(dst, dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
@@ -732,7 +757,7 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s)
     if (!ctx || !terms_per_s) return BPMAX_EINVAL;
     CK(cudaSetDevice(ctx->device));
     float *buf = nullptr;
-    const int grid = ctx->sms * 8, block = 128, reps = 4000;
+    const int grid = ctx->sms * 8, block = 128, reps = 1000;
     CK(cudaMalloc(&buf, (size_t)grid * block * sizeof(float) + 64 * sizeof(float)));
     std::vector<float> h(64);
     for (int i = 0; i < 64; ++i) h[i] = (float)(i % 17);
@@ -746,7 +771,7 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s)
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     cudaFree(buf);
     if (e != cudaSuccess) return fail(ctx, BPMAX_ECUDA, "peak probe: %s", cudaGetErrorString(e));
-    *terms_per_s = 3.0 * grid * block * (double)reps * 128.0 / (ms * 1e-3);
+    *terms_per_s = 3.0 * grid * block * (double)reps * 512.0 / (ms * 1e-3);
     return BPMAX_OK;
 }
 
@@ -780,6 +805,7 @@ static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_FLOATS];
 struct NoallocDevice {
     float *ptr = nullptr;  // device address of g_noalloc_scratch on this device
     int sms = 0;
+    int occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class
 };
 std::mutex g_noalloc_mu;
 constexpr int NOALLOC_MAX_DEVICES = 64;
@@ -795,20 +821,23 @@ __global__ void noalloc_prep_kernel(const int *__restrict__ seqs, int M, int N, 
     }
 }
 
-// R0 jobs of diagonal d: cells (i1, i1+d), k1 chunks of csize
-__global__ void noalloc_r0_jobs_kernel(R0Job *__restrict__ jobs, int cells, int d, int csize, int per_cell)
+// product jobs of diagonal d: pair chunk c of q offset pairs for every cell (i1, i1+d), ordered by
+// chunk then cell, as the context path orders them
+__global__ void noalloc_r0_jobs_kernel(R0Job *__restrict__ jobs, int cells, int d, int q, int njobs)
 {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= cells * per_cell) return;
-    const int i1 = q / per_cell, c = q % per_cell;
-    const int a = i1 + c * csize;
-    jobs[q] = R0Job{0, i1, a, min(a + csize, i1 + d)};
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= njobs) return;
+    const int P2 = (d + 1) / 2, c = t / cells, i1 = t % cells;
+    jobs[t] = R0Job{0, i1, c * q, min(c * q + q, P2)};
 }
 
 template <int NB>
-int noalloc_set_attr()
+int noalloc_set_attr(int *occ)
 {
-    if (cudaFuncSetAttribute(r0_small_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Shape<NB>::SMEM) !=
+    if (cudaFuncSetAttribute(r0_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM) !=
+        cudaSuccess)
+        return BPMAX_ECUDA;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[NB], r0_kernel<NB>, R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM) !=
         cudaSuccess)
         return BPMAX_ECUDA;
     return cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -829,14 +858,14 @@ int noalloc_setup(int dev, NoallocDevice *out)
         }
         int sms = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return BPMAX_ECUDA;
-        int st = noalloc_set_attr<1>();
-        if (!st) st = noalloc_set_attr<2>();
-        if (!st) st = noalloc_set_attr<3>();
-        if (!st) st = noalloc_set_attr<4>();
-        if (!st) st = noalloc_set_attr<5>();
-        if (!st) st = noalloc_set_attr<6>();
-        if (!st) st = noalloc_set_attr<7>();
-        if (!st) st = noalloc_set_attr<8>();
+        int st = noalloc_set_attr<1>(nd.occ);
+        if (!st) st = noalloc_set_attr<2>(nd.occ);
+        if (!st) st = noalloc_set_attr<3>(nd.occ);
+        if (!st) st = noalloc_set_attr<4>(nd.occ);
+        if (!st) st = noalloc_set_attr<5>(nd.occ);
+        if (!st) st = noalloc_set_attr<6>(nd.occ);
+        if (!st) st = noalloc_set_attr<7>(nd.occ);
+        if (!st) st = noalloc_set_attr<8>(nd.occ);
         if (st) return st;
         nd.sms = sms;
         nd.ptr = p;
@@ -846,15 +875,16 @@ int noalloc_setup(int dev, NoallocDevice *out)
 }
 
 template <int NB>
-void noalloc_launch_diag(cudaStream_t s, int sms, int d, int n_r0, int n_cells, const R0Job *rj, const CellJob *cj,
-                         const PairDesc *pd, float *F, float *FT, float *S, const uint8_t *bases, const Weights &W)
+void noalloc_launch_diag(cudaStream_t s, const NoallocDevice &nd, int d, int n_r0, int n_cells, const R0Job *rj,
+                         const CellJob *cj, const PairDesc *pd, float *F, float *S, const uint8_t *bases, const Weights &W,
+                         int *err)
 {
     if (d > 0)
-        r0_small_kernel<NB><<<std::min(n_r0, 3 * sms), R0Shape<NB>::THREADS, R0Shape<NB>::SMEM, s>>>(rj, n_r0, pd, F,
-                                                                                                 FT, S, d);
+        r0_kernel<NB><<<std::min(n_r0, std::max(1, nd.occ[NB]) * nd.sms), R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM, s>>>(
+            rj, n_r0, pd, F, d, err);
     const int n_s1 = n_cells - 1;  // S1 cells of diagonal d+1: the first n_cells-1 entries of cj
     finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + 3) / 4, 128, FinShape<8 * NB>::SMEM, s>>>(
-        cj, n_cells, cj, n_s1, pd, F, FT, S, bases, W, d);
+        cj, n_cells, cj, n_s1, pd, F, S, bases, W, d);
 }
 
 }  // namespace
@@ -872,14 +902,13 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     const int Np = std::max(8, (int)(N + 7) / 8 * 8);
     const int nb = Np / 8;
     // scratch layout (floats), every region 256-byte aligned
-    const long long nF = (long long)M * (M + 1) / 2 * Np * Np;
-    const long long off_FT = align64(nF);
-    const long long off_S = off_FT + align64(nF);
+    const long long nF = (long long)M * (M + 1) / 2 * cell_floats(Np);
+    const long long off_S = align64(nF);
     const long long S2_rel = align64((long long)M * M);
     const long long off_seq = off_S + align64(S2_rel + (long long)Np * Np);
     const long long off_bases = off_seq + align64(M + N);
     const long long off_pd = off_bases + align64((M + N + 3) / 4);
-    const long long off_score = off_pd + align64((long long)(sizeof(PairDesc) + 3) / 4);
+    const long long off_score = off_pd + align64((long long)(sizeof(PairDesc) + 3) / 4);  // score, error flag
     const long long off_cj = off_score + 64;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
@@ -889,18 +918,22 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     NoallocDevice nd;
     int st = noalloc_setup(dev, &nd);
     if (st) return st;
-    const int target = 4 * nd.sms;
+    const long long resident = (long long)std::max(1, nd.occ[nb]) * nd.sms;
+    const int qmin = std::max(1, (R0_TAB_ITEMS[nb] + 1) / 2);
+    // jobs per diagonal <= M * ceil(P2 / qmin) <= M * ((M + 1) / 2)
     const long long off_rj = off_cj + align64(2LL * M);
-    const long long total = off_rj + 4LL * (M + target + 1);
+    const long long max_jobs = (long long)M * (((M + 1) / 2 + qmin - 1) / qmin);
+    const long long total = off_rj + 4LL * max_jobs;
     if ((size_t)total > NOALLOC_FLOATS) return BPMAX_EINVAL;  // pair too large for the fixed scratch
 
     cudaStream_t s = (cudaStream_t)stream;
     float *base = nd.ptr;
-    float *F = base, *FT = base + off_FT, *S = base + off_S;
+    float *F = base, *S = base + off_S;
     int *seqs = reinterpret_cast<int *>(base + off_seq);
     uint8_t *bases = reinterpret_cast<uint8_t *>(base + off_bases);
     PairDesc *pdp = reinterpret_cast<PairDesc *>(base + off_pd);
     float *dscore = base + off_score;
+    int *derr = reinterpret_cast<int *>(base + off_score + 1);
     CellJob *cj = reinterpret_cast<CellJob *>(base + off_cj);
     R0Job *rj = reinterpret_cast<R0Job *>(base + off_rj);
     PairDesc pd{};
@@ -920,8 +953,9 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     if (!ok(cudaMemcpyAsync(seqs, seq1, sizeof(int) * M, cudaMemcpyHostToDevice, s)) ||
         !ok(cudaMemcpyAsync(seqs + M, seq2, sizeof(int) * N, cudaMemcpyHostToDevice, s)) ||
         !ok(cudaMemcpyAsync(pdp, &pd, sizeof pd, cudaMemcpyHostToDevice, s)) ||
-        !ok(cudaMemsetAsync(F, 0, sizeof(float) * nF, s)) ||  // F starts at +0 on every call
-        !ok(cudaMemsetAsync(S, 0, sizeof(float) * S2_rel, s))) {  // and S1 at 0
+        !ok(cudaMemsetAsync(F, 0, sizeof(float) * nF, s)) ||        // F starts at +0 on every call
+        !ok(cudaMemsetAsync(S, 0, sizeof(float) * S2_rel, s)) ||    // and S1 at 0
+        !ok(cudaMemsetAsync(derr, 0, sizeof(int), s))) {
         cudaGetLastError();
         return BPMAX_ECUDA;
     }
@@ -931,28 +965,32 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
         const int cells = (int)M - d;
         int n_r0 = 0;
         if (d > 0) {
-            const long long chunks = std::max(1LL, std::min((long long)d, (long long)(target + cells - 1) / cells));
-            const int csize = (int)((d + chunks - 1) / chunks);
-            const int per_cell = (d + csize - 1) / csize;
-            n_r0 = cells * per_cell;
-            noalloc_r0_jobs_kernel<<<(n_r0 + 255) / 256, 256, 0, s>>>(rj, cells, d, csize, per_cell);
+            const long long P2 = (d + 1) / 2;
+            const long long q = std::max<long long>(qmin, (cells * P2 + 2 * resident - 1) / (2 * resident));
+            n_r0 = (int)(cells * ((P2 + q - 1) / q));
+            noalloc_r0_jobs_kernel<<<(n_r0 + 255) / 256, 256, 0, s>>>(rj, cells, d, (int)q, n_r0);
         }
         switch (nb) {
-        case 1: noalloc_launch_diag<1>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 2: noalloc_launch_diag<2>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 3: noalloc_launch_diag<3>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 4: noalloc_launch_diag<4>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 5: noalloc_launch_diag<5>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 6: noalloc_launch_diag<6>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        case 7: noalloc_launch_diag<7>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
-        default: noalloc_launch_diag<8>(s, nd.sms, d, n_r0, cells, rj, cj, pdp, F, FT, S, bases, W); break;
+        case 1: noalloc_launch_diag<1>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        case 2: noalloc_launch_diag<2>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        case 3: noalloc_launch_diag<3>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        case 4: noalloc_launch_diag<4>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        case 5: noalloc_launch_diag<5>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        case 6: noalloc_launch_diag<6>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        case 7: noalloc_launch_diag<7>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
+        default: noalloc_launch_diag<8>(s, nd, d, n_r0, cells, rj, cj, pdp, F, S, bases, W, derr); break;
         }
     }
     gather_scores_kernel<<<1, 32, 0, s>>>(pdp, F, 1, dscore);
-    if (!ok(cudaGetLastError()) || !ok(cudaMemcpyAsync(score, dscore, sizeof(float), cudaMemcpyDeviceToHost, s)) ||
+    float out[2] = {0.f, 0.f};  // score, error flag bits
+    if (!ok(cudaGetLastError()) || !ok(cudaMemcpyAsync(out, dscore, 2 * sizeof(float), cudaMemcpyDeviceToHost, s)) ||
         !ok(cudaStreamSynchronize(s))) {
         cudaGetLastError();
         return BPMAX_ECUDA;
     }
+    int errbits = 0;
+    memcpy(&errbits, &out[1], sizeof errbits);
+    if (errbits != 0) return BPMAX_ETIMEOUT;
+    *score = out[0];
     return BPMAX_OK;
 }

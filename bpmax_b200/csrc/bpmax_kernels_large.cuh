@@ -6,6 +6,60 @@
 namespace bpmax {
 
 // ------------------------------------------------------------------------------------------
+// Shared-memory stage of the wide product kernel: rows k' = 0..64 of the shifted A operand
+// (A_s^T[k'][i2], 64 columns i2 of one output block) and of B (B[k'][j2], 64 columns j2), rows
+// unpadded and XOR-swizzled per 16-byte chunk so that the task table below is conflict-free.
+// ------------------------------------------------------------------------------------------
+struct WideShape {
+    static constexpr int NP = 64;
+    static constexpr int LD = NP;                     // row stride (floats)
+    static constexpr int ROWS = NP + 1;
+    static constexpr int A_FLOATS = ROWS * LD;        // A_s^T[k'][i2], k' = 0..NP
+    static constexpr int STAGE = 2 * A_FLOATS;        // + B[k'][j2], k' = 0..NP
+    static constexpr int TASKS = 120;                 // (bi, bj, kb), bi <= kb <= bj < 8
+    static constexpr size_t SMEM = 2 * (size_t)STAGE * sizeof(float);
+};
+
+// shared offset (floats) of row r, column c (c a multiple of 4 for 16-byte accesses)
+__device__ __forceinline__ int wide_off(int r, int c)
+{
+    const int cc = c >> 2;
+    const int pc = cc ^ (cc >> 3) ^ (((r >> 3) & 3) << 1);
+    return r * WideShape::LD + (pc << 2) + (c & 3);
+}
+
+// task (bi, bj, kb) of each lane for a 64x64 diagonal output block: 15 quarter-warps whose 128-bit
+// shared loads of A and B hit 8 distinct bank groups (or one broadcast address) under wide_off's
+// swizzle; lanes 120..127 idle.
+__constant__ unsigned char c_wide_lane[120][3] = {
+    {0,2,0},{0,6,0},{0,5,0},{0,4,0},{0,0,0},{0,1,0},{0,7,0},{0,3,0},{1,4,1},{0,5,1},{0,7,1},{0,4,1},
+    {0,6,1},{1,2,1},{1,7,1},{1,5,1},{0,2,2},{0,3,2},{2,5,2},{1,6,2},{1,5,2},{0,7,2},{1,2,2},{0,6,2},
+    {2,7,2},{0,4,2},{2,3,2},{1,4,2},{2,2,2},{2,4,2},{2,6,2},{1,7,2},{2,3,3},{2,7,3},{1,7,3},{3,5,3},
+    {3,7,3},{0,3,3},{1,4,3},{3,3,3},{2,5,3},{0,4,3},{0,7,3},{3,6,3},{2,6,3},{3,4,3},{2,4,3},{0,6,3},
+    {2,7,4},{2,5,4},{0,7,4},{0,5,4},{1,7,4},{1,4,4},{1,6,4},{3,7,4},{0,6,4},{0,4,4},{4,4,4},{2,6,4},
+    {3,4,4},{3,6,4},{2,4,4},{3,5,4},{5,6,5},{4,6,5},{2,7,5},{1,7,5},{5,7,5},{2,6,5},{1,6,5},{3,5,5},
+    {0,6,5},{5,5,5},{3,6,5},{0,5,5},{2,5,5},{3,7,5},{4,7,5},{0,7,5},{4,7,6},{6,6,6},{6,7,6},{0,7,6},
+    {0,6,6},{2,6,6},{3,6,6},{3,7,6},{0,7,7},{4,7,7},{3,7,7},{2,7,7},{1,7,7},{7,7,7},{5,7,7},{6,7,7},
+    {0,2,1},{0,3,1},{1,3,1},{1,1,1},{0,1,1},{1,6,1},{1,3,2},{1,6,3},{0,5,2},{4,6,4},{2,7,6},{1,6,6},
+    {1,7,6},{4,6,6},{5,6,6},{5,7,6},{1,3,3},{1,5,3},{0,5,3},{1,5,4},{4,5,4},{4,7,4},{1,5,5},{4,5,5}};
+
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+
+// ------------------------------------------------------------------------------------------
 // Masked copies of S2 for the large finalize: S2M[i][k] = S2(i,k) if i <= k < N else -inf and
 // ST1[j][k] = S2(k+1,j) if k+1 <= j < N else -inf (S2 over the reversed strand 2,
 // V3/bpmax_verify.c:560-571). One CTA per pair; pairs with Np <= 64 are skipped.
@@ -25,12 +79,14 @@ __global__ void s2_aux_kernel(const PairDesc *__restrict__ pairs, float *__restr
 }
 
 // ------------------------------------------------------------------------------------------
-// R0 + R3 + R4 (same triangular (max,+) product as r0_small_kernel: A_s = F(i1,k1) shifted one
-// column right with S1(i1,k1) on its diagonal, B = F(k1+1,j1) with S1(k1+1,j1) on its
-// subdiagonal) for Np = 64*NBk. A job is one outer cell, one 64x64 output block (BI,BJ) and a k1
+// R0 + R3 + R4 for Np = 64*NBk (row-major F and its transpose FT, Np x Np per outer cell). With
+// A_s = F(i1,k1) shifted one column right (A_s[i2][k'] = F(i1,k1)[i2][k'-1], A_s[0][0] =
+// S1(i1,k1)) and B = F(k1+1,j1) (S1(k1+1,j1) on its subdiagonal, guard row Np = S1(k1+1,j1) at
+// column Np-1), R0, R3 and R4 are one triangular (max,+) product max_{k' in [i2, j2+1]}
+// A_s[i2][k'] + B[k'][j2]. A job is one outer cell, one 64x64 output block (BI,BJ) and a k1
 // range; it loops over the k' blocks KB in [BI, BJ]. Each stage holds rows k' = 64KB..64KB+64 of
-// A_s (columns i2 of block BI) and of B (columns j2 of block BJ) in the swizzled 64-wide layout
-// of r0_small_kernel<8>. Diagonal output blocks use its balanced triangular task table; the
+// A_s (columns i2 of block BI, read from FT) and of B (columns j2 of block BJ) in WideShape's
+// layout. Diagonal output blocks use the balanced triangular task table c_wide_lane; the
 // other blocks give every thread one 8x8 micro-tile and half of the eight 8-wide k' sub-blocks
 // (A is triangular in the stage KB == BI, B in the stage KB == BJ, dense in between).
 // ------------------------------------------------------------------------------------------
@@ -42,7 +98,7 @@ __global__ void __launch_bounds__(128, 3)
 r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs, float *__restrict__ F,
                 const float *__restrict__ FT, const float *__restrict__ S, int d)
 {
-    using Sh = R0Shape<8>;
+    using Sh = WideShape;
     constexpr int B = 64;
     extern __shared__ __align__(16) float smem[];
     const int tid = threadIdx.x;
@@ -66,17 +122,17 @@ r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__re
                 if (kp == 0) {  // A_s row 0: S1(i1,k1) at (0,0), -inf elsewhere
                     float4 v = make_float4(NEG_INF, NEG_INF, NEG_INF, NEG_INF);
                     if (BI == 0 && cc == 0) v.x = S1[jb.i1 * M + k1];
-                    *reinterpret_cast<float4 *>(st + r0_off<8>(r, 4 * cc)) = v;
+                    *reinterpret_cast<float4 *>(st + wide_off(r, 4 * cc)) = v;
                 } else {
-                    cp_async16(st + r0_off<8>(r, 4 * cc), ga + (long long)(kp - 1) * Np + B * BI + 4 * cc);
+                    cp_async16(st + wide_off(r, 4 * cc), ga + (long long)(kp - 1) * Np + B * BI + 4 * cc);
                 }
             } else {
                 if (kp == Np) {  // guard row: S1(k1+1,j1) at (Np, Np-1), -inf elsewhere
                     float4 v = make_float4(NEG_INF, NEG_INF, NEG_INF, NEG_INF);
                     if (BJ == NBk - 1 && cc == 15) v.w = S1[(k1 + 1) * M + j1];
-                    *reinterpret_cast<float4 *>(st + Sh::A_FLOATS + r0_off<8>(r, 4 * cc)) = v;
+                    *reinterpret_cast<float4 *>(st + Sh::A_FLOATS + wide_off(r, 4 * cc)) = v;
                 } else {
-                    cp_async16(st + Sh::A_FLOATS + r0_off<8>(r, 4 * cc), gb + (long long)kp * Np + B * BJ + 4 * cc);
+                    cp_async16(st + Sh::A_FLOATS + wide_off(r, 4 * cc), gb + (long long)kp * Np + B * BJ + 4 * cc);
                 }
             }
         }
@@ -91,8 +147,8 @@ r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__re
     bool has_task = false;
     auto map_threads = [&]() {
         if (BI == BJ) {
-            has_task = tid < R0Shape<8>::TASKS;
-            if (has_task) { bi = c_r0_lane64[tid][0]; bj = c_r0_lane64[tid][1]; kb = c_r0_lane64[tid][2]; }
+            has_task = tid < WideShape::TASKS;
+            if (has_task) { bi = c_wide_lane[tid][0]; bj = c_wide_lane[tid][1]; kb = c_wide_lane[tid][2]; }
         } else {
             has_task = true;
             const int m = tid & 63;
@@ -112,14 +168,14 @@ r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__re
 #pragma unroll
         for (int k = 0; k < 8; k += 2) {
             const int r = 8 * kbl + k;
-            const float4 a0 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi));
-            const float4 a1 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi + 4));
-            const float4 a2 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r + 1, 8 * bi));
-            const float4 a3 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r + 1, 8 * bi + 4));
-            const float4 b0 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r, 8 * bj));
-            const float4 b1 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r, 8 * bj + 4));
-            const float4 b2 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r + 1, 8 * bj));
-            const float4 b3 = *reinterpret_cast<const float4 *>(Bs + r0_off<8>(r + 1, 8 * bj + 4));
+            const float4 a0 = *reinterpret_cast<const float4 *>(As + wide_off(r, 8 * bi));
+            const float4 a1 = *reinterpret_cast<const float4 *>(As + wide_off(r, 8 * bi + 4));
+            const float4 a2 = *reinterpret_cast<const float4 *>(As + wide_off(r + 1, 8 * bi));
+            const float4 a3 = *reinterpret_cast<const float4 *>(As + wide_off(r + 1, 8 * bi + 4));
+            const float4 b0 = *reinterpret_cast<const float4 *>(Bs + wide_off(r, 8 * bj));
+            const float4 b1 = *reinterpret_cast<const float4 *>(Bs + wide_off(r, 8 * bj + 4));
+            const float4 b2 = *reinterpret_cast<const float4 *>(Bs + wide_off(r + 1, 8 * bj));
+            const float4 b3 = *reinterpret_cast<const float4 *>(Bs + wide_off(r + 1, 8 * bj + 4));
             const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
             const float aw[8] = {a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
             const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
@@ -132,9 +188,9 @@ r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__re
     };
     auto edge_step = [&](const float *As, const float *Bs) {  // k' = 8bj+8 (local): R4 of column 8bj+7
         const int r = 8 * bj + 8;
-        const float4 a0 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi));
-        const float4 a1 = *reinterpret_cast<const float4 *>(As + r0_off<8>(r, 8 * bi + 4));
-        const float bs = Bs[r0_off<8>(r, 8 * bj + 4) + 3];
+        const float4 a0 = *reinterpret_cast<const float4 *>(As + wide_off(r, 8 * bi));
+        const float4 a1 = *reinterpret_cast<const float4 *>(As + wide_off(r, 8 * bi + 4));
+        const float bs = Bs[wide_off(r, 8 * bj + 4) + 3];
         const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
 #pragma unroll
         for (int i = 0; i < 8; ++i) acc[i][7] = fmaxf(acc[i][7], av[i] + bs);

@@ -1,0 +1,311 @@
+// bpmax_r0.cuh -- R0 + R3 + R4 product kernel for inner tables of width Np = 8*NB <= 64.
+//
+// For one outer cell (i1, j1 = i1+d) and one k1 in [i1, j1) (an "item"), with A = F(i1,k1) and
+// B = F(k1+1,j1) (tables whose subdiagonal holds S1 of their own cell):
+//   R0 (V3/bpmax_verify.c:584-613):  max_{k2 in [i2, j2)} A[i2][k2] + B[k2+1][j2]
+//   R3 (:668-694):                    S1(i1,k1) + B[i2][j2]      = A[i2][i2-1] + B[i2][j2]
+//   R4 (:695-721):                    A[i2][j2] + S1(k1+1,j1)    = A[i2][j2]   + B[j2+1][j2]
+// With the row-shifted operand Bs[k][j] = B[k+1][j] all three are one triangular (max,+) product
+//   max_{k in [i2-1, j2]} A[i2][k] + Bs[k][j2]
+// (every other k meets a -inf below a diagonal). It is split into tasks (bi, bj, kb),
+// bi <= kb <= bj: the 8x8 output micro-tile (bi, bj) times the k block [8kb, 8kb+8); a task with
+// kb == bi also adds the k = 8bi-1 term of its first row (S1(i1,k1) + B[8bi][j2]), which lies
+// outside every k block of the micro-tile.
+//
+// Data movement: the stored inner table of a cell is a "cell image" (bpmax_kernels.cuh): block
+// columns of 8x8 blocks at a pitch of 17 16-byte chunks, each column closed by its S1 piece. An
+// item needs exactly two whole images in shared memory, A = F(i1,k1) and B = F(k1+1,j1): two bulk
+// copies on the TMA engine (cp.async.bulk, completion counted on the stage's mbarrier). In the
+// images, A block (bi,kb) is column kb, block bi; the shifted B block (kb,bj) is rows 1..7 of
+// block kb of column bj followed by row 0 of block kb+1 (or, for kb == bj, the column's S1 piece,
+// which is exactly row 8kb+8 of B below the block diagonal and, in the last column, the guard row
+// B[Np]); the R3 row B[8bi] is row 0 of block bi of column bj. The column pads and the lane ->
+// task table (r0_tables.inc) make every quarter-warp's 128-bit loads hit distinct bank groups.
+// Stages form a ring; one CTA barrier per iteration frees the stage the next copies overwrite.
+// Both operands are whole images of the same F tables, so the two uses of a table on one
+// diagonal (as A of cell (a, a+d) and as B of cell (b-d, b)) can meet in L2: jobs visit k1
+// offsets in pairs (w, d-1-w), the offset pair p = min(w, d-1-w) being the same for both uses,
+// and the job list is ordered by offset pair.
+//
+// The inner loop adds in pairs: (a, a) + (b[j], b[j+1]) with one packed fp32 add (__fadd2_rn,
+// round-to-nearest like the scalar add), and merges four candidates per accumulator with two
+// 3-input max steps. At the end of a job the partial maxima of all tasks first meet in a shared
+// tile of the cell's blocks (shared atomicMax; blocks at a pitch of 65 words so the lanes of a
+// warp hit distinct banks), then the tile merges into F(i1, j1) with coalesced global atomicMax,
+// consecutive lanes on consecutive words (max on the int bit patterns is exact: all values are
+// >= +0; -inf partials and +0 entries are skipped).
+#pragma once
+#include <cstdint>
+
+#include "bpmax_kernels.cuh"
+
+namespace bpmax {
+
+// one job: cell (i1, i1+d) of pair `pair`, k1 offset pairs p in [p0, p1) (offsets w = p and d-1-p)
+struct R0Job {
+    int pair, i1, p0, p1;
+};
+
+__host__ __device__ __forceinline__ int r0_job_items(const R0Job &j, int d)
+{
+    const int P = (d + 1) / 2;
+    return 2 * (j.p1 - j.p0) - (((d & 1) && j.p1 == P) ? 1 : 0);
+}
+__host__ __device__ __forceinline__ int r0_item_offset(const R0Job &j, int d, int n)
+{
+    const int p = j.p0 + (n >> 1);
+    return (n & 1) ? d - 1 - p : p;
+}
+
+template <int NB>
+struct R0Cfg {
+    static constexpr int NP = 8 * NB;
+    static constexpr int THREADS = R0_TAB_THREADS[NB];
+    static constexpr int G = R0_TAB_ITEMS[NB];              // items per iteration
+    static constexpr int IMG = R0_TAB_COLBASE[NB][NB];      // chunks per cell image
+    static constexpr int ITEM = 2 * IMG + R0_TAB_IPAD[NB];  // A image, B image, pad (chunks)
+    static constexpr int STAGE = G * ITEM;                  // chunks
+    static constexpr int STAGE_BYTES = STAGE * 16;
+    static constexpr int NBLK = NB * (NB + 1) / 2;
+    static constexpr int RED_WORDS = 65 * NBLK;             // job-merge tile, one 8x8 block per 65 words
+    static constexpr int STAGE_BUDGET = 75 * 1024 - 4 * RED_WORDS - 4 * NBLK - 64;  // 3 CTAs per SM
+    static constexpr int STAGES = STAGE_BYTES * 4 <= STAGE_BUDGET ? 4 : (STAGE_BYTES * 3 <= STAGE_BUDGET ? 3 : 2);
+    static constexpr int ITEM_TX = 2 * IMG * 16;            // bytes landing per item
+    static constexpr int MINB = THREADS <= 64 ? 6 : (THREADS <= 96 ? 4 : 3);
+    // shared memory: stages, merge tile, block offsets, one mbarrier per stage (byte offsets)
+    static constexpr int OFF_RED = STAGES * STAGE_BYTES;
+    static constexpr int OFF_DST = OFF_RED + 4 * RED_WORDS;
+    static constexpr int OFF_BAR = (OFF_DST + 4 * NBLK + 15) / 16 * 16;
+    static constexpr size_t SMEM = (size_t)OFF_BAR + 8 * STAGES;
+    static_assert(STAGE_BYTES % 16 == 0 && OFF_RED % 16 == 0 && OFF_BAR % 8 == 0, "shared-memory alignment");
+    static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// bounded wait for the completion of phase `parity` of an mbarrier; false when the bound ran out
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+{
+    for (int tries = 0; tries < (1 << 24); ++tries) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+// global -> shared bulk copy on the TMA engine (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+template <int NB>
+__global__ void __launch_bounds__(R0Cfg<NB>::THREADS, R0Cfg<NB>::MINB)
+r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs, float *__restrict__ F, int d,
+          int *__restrict__ err)
+{
+    using C = R0Cfg<NB>;
+    constexpr int S = C::STAGES;
+    constexpr long long CELL = 4LL * C::IMG;
+    extern __shared__ __align__(128) float r0sm[];
+    float *smem = r0sm;
+    int *red = reinterpret_cast<int *>(reinterpret_cast<char *>(smem) + C::OFF_RED);      // job-merge tile
+    int *red_dst = reinterpret_cast<int *>(reinterpret_cast<char *>(smem) + C::OFF_DST);  // float offset of each
+                                                                                          // block in a cell image
+    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(smem) + C::OFF_BAR);
+    const int tid = threadIdx.x;
+    int jid = blockIdx.x;
+    if (jid >= njobs) return;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(smem_u32(bars + s), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int q = tid; q < C::RED_WORDS; q += C::THREADS) red[q] = 0;  // +0: below every partial maximum
+    if (tid < C::NBLK) {
+        int bi_ = 0, bj_ = tid;
+        while (bj_ >= NB - bi_) { bj_ -= NB - bi_; ++bi_; }
+        bj_ += bi_;
+        red_dst[tid] = 4 * (c_img_colbase[NB][bj_] + 17 * bi_);
+    }
+
+    // this thread's task and its float offsets inside an item
+    const unsigned char *lt = c_r0_lane[NB - 1][tid];
+    const bool has_task = lt[0] != 255;
+    const int tg = has_task ? lt[0] : 0, bi = lt[1], bj = lt[2], kb = lt[3];
+    int a_off = 0, b_off = 0, r3_off = 0, red_off = 0;
+    if (has_task) {
+        red_off = 65 * (bi * NB - bi * (bi - 1) / 2 + (bj - bi));       // block (bi, bj) of the merge tile
+        a_off = 4 * (c_img_colbase[NB][kb] + 17 * bi);                 // A block (bi, kb), row 0
+        b_off = 4 * (C::IMG + c_img_colbase[NB][bj] + 17 * kb + 2);     // shifted B block (kb, bj), row 0
+        r3_off = 4 * (C::IMG + c_img_colbase[NB][bj] + 17 * bi);        // B row 8bi, columns 8bj..
+    }
+    constexpr int s1_off = 8;  // A[1][0] = S1(i1,k1): column 0, block 0, row 1
+    __syncthreads();  // mbarrier init visible
+
+    const unsigned smem_base = smem_u32(smem);
+    // announces the bytes of iteration `it` of job `jb` on stage s's mbarrier (thread 0 only; done
+    // before the CTA barrier that precedes the copies, so no copy can complete before it)
+    auto expect = [&](int s, const R0Job &jb, int it) {
+        const int valid = min(C::G, r0_job_items(jb, d) - it * C::G);
+        mbar_arrive_tx(smem_u32(bars + s), (unsigned)(valid * C::ITEM_TX));
+    };
+    // issues this thread's copies (whole cell images) of iteration `it` of job `jb` into stage s
+    auto issue = [&](int s, const R0Job &jb, int it) {
+        const PairDesc pd = pairs[jb.pair];
+        const int M = pd.M, j1 = jb.i1 + d;
+        const int valid = min(C::G, r0_job_items(jb, d) - it * C::G);
+        const unsigned bar = smem_u32(bars + s);
+        const float *Fp = F + pd.F_off;
+        for (int o = tid; o < 2 * valid; o += C::THREADS) {
+            const int g = o >> 1, k1 = jb.i1 + r0_item_offset(jb, d, it * C::G + g);
+            const long long cell = (o & 1) ? cell_index(M, k1 + 1, j1) : cell_index(M, jb.i1, k1);
+            bulk_g2s(smem_base + (unsigned)(s * C::STAGE_BYTES + (g * C::ITEM + (o & 1) * C::IMG) * 16), Fp + cell * CELL,
+                     (unsigned)(C::IMG * 16), bar);
+        }
+    };
+
+    // consumer position (jid, job, it) and producer position (pj, pjob, pit), S-1 iterations ahead
+    R0Job job = jobs[jid];
+    int n_it = (r0_job_items(job, d) + C::G - 1) / C::G, it = 0;
+    int pj = jid, pit = 0;
+    R0Job pjob = job;
+    auto advance = [&](int &j_, R0Job &jb_, int &it_) {
+        if (++it_ * C::G >= r0_job_items(jb_, d)) {
+            it_ = 0;
+            j_ += gridDim.x;
+            if (j_ < njobs) jb_ = jobs[j_];
+        }
+    };
+    if (tid == 0) {  // expected bytes of the first S-1 iterations and of the first in-loop issue
+        int j_ = pj, it_ = pit;
+        R0Job jb_ = pjob;
+        for (int s = 0; s < S && j_ < njobs; ++s) {
+            expect(s, jb_, it_);
+            advance(j_, jb_, it_);
+        }
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int s = 0; s < S - 1; ++s)
+        if (pj < njobs) {
+            issue(s, pjob, pit);
+            advance(pj, pjob, pit);
+        }
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = NEG_INF;
+
+    unsigned phase = 0;  // bit s: parity of stage s's next completion
+    int stage = 0;
+    bool bad = false;
+#pragma unroll 1
+    while (true) {
+        // every thread is done with the previous iteration: its stage may be refilled
+        if (__syncthreads_or(bad)) return;
+        if (pj < njobs) {
+            issue((stage + S - 1) % S, pjob, pit);
+            advance(pj, pjob, pit);
+        }
+        const bool active = has_task && it * C::G + tg < r0_job_items(job, d);
+        if (!mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u)) {
+            atomicExch(err, 1);
+            bad = true;
+            continue;  // leave together at the next CTA barrier
+        }
+        phase ^= 1u << stage;
+        if (active) {
+            const float *item = smem + (size_t)stage * C::STAGE * 4 + tg * C::ITEM * 4;
+            const float *As = item + a_off, *Bs = item + b_off;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                float av[8][4];
+                float2 bv[4][4];  // bv[k][jp] = (Bs[4q+k][2jp], Bs[4q+k][2jp+1])
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float4 t = *reinterpret_cast<const float4 *>(As + 8 * i + 4 * q);
+                    av[i][0] = t.x; av[i][1] = t.y; av[i][2] = t.z; av[i][3] = t.w;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int row = 4 * q + k, ro = 8 * row + (row == 7 ? 4 : 0);  // row 7: next block / S1 piece
+                    const float4 t0 = *reinterpret_cast<const float4 *>(Bs + ro);
+                    const float4 t1 = *reinterpret_cast<const float4 *>(Bs + ro + 4);
+                    bv[k][0] = make_float2(t0.x, t0.y); bv[k][1] = make_float2(t0.z, t0.w);
+                    bv[k][2] = make_float2(t1.x, t1.y); bv[k][3] = make_float2(t1.z, t1.w);
+                }
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int jp = 0; jp < 4; ++jp) {
+                        const float2 s0 = __fadd2_rn(make_float2(av[i][0], av[i][0]), bv[0][jp]);
+                        const float2 s1 = __fadd2_rn(make_float2(av[i][1], av[i][1]), bv[1][jp]);
+                        const float2 s2 = __fadd2_rn(make_float2(av[i][2], av[i][2]), bv[2][jp]);
+                        const float2 s3 = __fadd2_rn(make_float2(av[i][3], av[i][3]), bv[3][jp]);
+                        acc[i][2 * jp] = fmax3(fmax3(acc[i][2 * jp], s0.x, s1.x), s2.x, s3.x);
+                        acc[i][2 * jp + 1] = fmax3(fmax3(acc[i][2 * jp + 1], s0.y, s1.y), s2.y, s3.y);
+                    }
+            }
+            if (kb == bi) {  // k = 8bi-1 term of row 8bi: S1(i1,k1) + B[8bi][j2]
+                const float s1a = item[s1_off];
+                const float4 r0 = *reinterpret_cast<const float4 *>(item + r3_off);
+                const float4 r1 = *reinterpret_cast<const float4 *>(item + r3_off + 4);
+                const float rv[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[0][j] = fmaxf(acc[0][j], s1a + rv[j]);
+            }
+        }
+        // bytes of the next iteration's copies, which refill this stage (thread 0 has finished
+        // waiting on its current phase; the copies start only after the next CTA barrier)
+        if (tid == 0 && pj < njobs) expect(stage, pjob, pit);
+        if (++it >= n_it) {  // job done: merge the partial maxima of all tasks into F(i1, i1+d)
+            const PairDesc pd = pairs[job.pair];
+            if (has_task) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int i2 = 8 * bi + i, j2 = 8 * bj + j;
+                        const int v = __float_as_int(acc[i][j]);
+                        if (i2 <= j2 && j2 < pd.N && v > 0) atomicMax(red + red_off + 8 * i + j, v);
+                        acc[i][j] = NEG_INF;
+                    }
+            }
+            __syncthreads();
+            int *out = reinterpret_cast<int *>(F + pd.F_off + cell_index(pd.M, job.i1, job.i1 + d) * CELL);
+            for (int e = tid; e < 64 * C::NBLK; e += C::THREADS) {
+                const int q = e >> 6, w = e & 63;
+                const int v = red[65 * q + w];
+                if (v > 0) {
+                    atomicMax(out + red_dst[q] + w, v);
+                    red[65 * q + w] = 0;
+                }
+            }
+            jid += gridDim.x;
+            if (jid >= njobs) break;
+            job = jobs[jid];
+            n_it = (r0_job_items(job, d) + C::G - 1) / C::G;
+            it = 0;
+        }
+        stage = (stage + 1) % S;
+    }
+}
+
+}  // namespace bpmax

@@ -1,0 +1,152 @@
+#!/usr/bin/env python
+"""Generates r0_tables.inc: the cell-image layout constants and the lane -> task tables of the R0
+product kernel (bpmax_r0.cuh), one set per inner width class NB = 1..8 (inner width Np = 8*NB).
+
+Cell image (the stored inner table of one outer cell, in 16-byte chunks): block columns
+BJ = 0..NB-1 in turn; column BJ holds the 8x8 blocks (0..BJ, BJ) at a pitch of 17 chunks (8 rows
+of 2 chunks + 1 spare chunk), then the column's 2-chunk S1 piece, then colpad[BJ] spare chunks.
+The product kernel copies two whole images per item into shared memory (the A and the B
+operand). A lane's task (bi, bj, kb) reads
+  A block (bi, kb):          image A, column kb, block bi, rows i = 0..7
+  shifted B block (kb, bj):  image B, column bj, rows 1..7 of block kb then row 0 of block kb+1
+                             (or the column's S1 piece when kb == bj)
+  R3 row (kb == bi):         image B, column bj, row 0 of block bi
+each with one base register plus immediate offsets. A 128-bit shared load of a warp is served per
+quarter-warp (8 lanes); it takes one wavefront when the distinct 16-byte addresses of those lanes
+fall in distinct bank groups (address mod 8, in chunks). This script searches, with a seeded local
+search, the column pads, the item pad and the lane order that minimise the wavefronts of every
+load instruction of the inner loop and of the R3 step.
+
+    python bpmax_b200/csrc/gen_r0_tables.py   # rewrites bpmax_b200/csrc/r0_tables.inc
+"""
+from __future__ import annotations
+
+import os
+import random
+
+# (threads per CTA, items per iteration) for each NB: G*TASKS(NB) lanes work, the rest idle
+CFG = {1: (64, 64), 2: (96, 24), 3: (128, 12), 4: (128, 6), 5: (128, 3), 6: (128, 2), 7: (96, 1), 8: (128, 1)}
+
+
+def tasks(nb):
+    return [(bi, bj, kb) for bi in range(nb) for bj in range(bi, nb) for kb in range(bi, bj + 1)]
+
+
+class Layout:
+    """Chunk addresses of one stage: G items, each an A image then a B image, then ipad chunks."""
+
+    def __init__(self, nb, pads, ipad):
+        self.cb = []
+        o = 0
+        for c in range(nb):
+            self.cb.append(o)
+            o += 17 * (c + 1) + 2 + pads[c]
+        self.img = o
+        self.item = 2 * o + ipad
+
+    def a(self, g, bi, kb, i, q):
+        return g * self.item + self.cb[kb] + 17 * bi + 2 * i + q
+
+    def b(self, g, kb, bj, k, h):
+        return g * self.item + self.img + self.cb[bj] + 17 * kb + 2 + 2 * k + (1 if k == 7 else 0) + h
+
+    def r3(self, g, bi, bj, h):
+        return g * self.item + self.img + self.cb[bj] + 17 * bi + h
+
+
+def wavefronts(addrs):
+    groups = {}
+    for x in set(addrs):
+        groups.setdefault(x % 8, set()).add(x)
+    return max(len(v) for v in groups.values()) if groups else 0
+
+
+def cost(lay, lanes):
+    tot = 0
+    for qw in range(len(lanes) // 8):
+        sel = [x for x in lanes[qw * 8:qw * 8 + 8] if x is not None]
+        if not sel:
+            continue
+        for i in range(8):
+            for q in range(2):
+                tot += wavefronts([lay.a(g, t[0], t[2], i, q) for g, t in sel])
+        for k in range(8):
+            for h in range(2):
+                tot += wavefronts([lay.b(g, t[2], t[1], k, h) for g, t in sel])
+        r3 = [(g, t) for g, t in sel if t[2] == t[0]]
+        for h in range(2):
+            tot += wavefronts([lay.r3(g, t[0], t[1], h) for g, t in r3])
+    return tot
+
+
+def search(nb, iters, seed):
+    threads, G = CFG[nb]
+    rnd = random.Random(seed)
+    ts = sorted(tasks(nb), key=lambda t: (t[2], t[0], t[1]))
+    lanes = [(g, t) for g in range(G) for t in ts] + [None] * (threads - G * len(ts))
+    pads, ipad = [0] * nb, 0
+    lay = Layout(nb, pads, ipad)
+    cur = cost(lay, lanes)
+    for _ in range(iters):
+        if rnd.random() < 0.2:
+            c = rnd.randrange(nb + 1)
+            old = (pads[:], ipad)
+            if c == nb:
+                ipad = rnd.randrange(8)
+            else:
+                pads[c] = rnd.randrange(8)
+            lay2 = Layout(nb, pads, ipad)
+            cc = cost(lay2, lanes)
+            if cc <= cur:
+                cur, lay = cc, lay2
+            else:
+                pads, ipad = old
+        else:
+            x, y = rnd.randrange(threads), rnd.randrange(threads)
+            if x // 8 == y // 8:
+                continue
+            lanes[x], lanes[y] = lanes[y], lanes[x]
+            cc = cost(lay, lanes)
+            if cc <= cur:
+                cur = cc
+            else:
+                lanes[x], lanes[y] = lanes[y], lanes[x]
+    return cur, lanes, pads, ipad
+
+
+def main():
+    out = ["// r0_tables.inc -- generated by gen_r0_tables.py (seeded search); do not edit by hand.\n",
+           "// Per inner width class NB = 1..8: threads per CTA, items per iteration, spare chunks after each\n",
+           "// block column of a cell image and after each shared-memory item, and lane -> (item slot g, bi,\n",
+           "// bj, kb) (0xFF = idle lane).\n"]
+    T, G, P, colpad, colbase, lane_rows = [], [], [], [], [], []
+    for nb in range(1, 9):
+        c, lanes, pads, ipad = search(nb, 30000, nb)
+        threads, g = CFG[nb]
+        T.append(threads)
+        G.append(g)
+        P.append(ipad)
+        colpad.append("{" + ",".join(map(str, pads + [0] * (8 - nb))) + "}")
+        lay = Layout(nb, pads, ipad)
+        colbase.append("{" + ",".join(map(str, lay.cb + [lay.img] * (9 - nb))) + "}")
+        rows = ["{255,255,255,255}" if x is None else "{%d,%d,%d,%d}" % (x[0], *x[1])
+                for x in lanes + [None] * (256 - len(lanes))]
+        lane_rows.append("{" + ",".join(rows) + "}")
+        out.append(f"//   NB={nb}: {threads} threads, {g} items, search cost {c} wavefronts\n")
+    out.append("constexpr int R0_TAB_THREADS[9] = {0," + ",".join(map(str, T)) + "};\n")
+    out.append("constexpr int R0_TAB_ITEMS[9] = {0," + ",".join(map(str, G)) + "};\n")
+    out.append("constexpr int R0_TAB_IPAD[9] = {0," + ",".join(map(str, P)) + "};\n")
+    out.append("constexpr unsigned char R0_TAB_COLPAD[9][8] = {{0,0,0,0,0,0,0,0}," + ",".join(colpad) + "};\n")
+    out.append("// chunk offset of block column c (c = NB: the image size, in chunks) of a cell image\n")
+    cbt = "{{0,0,0,0,0,0,0,0,0}," + ",".join(colbase) + "}"
+    out.append("constexpr int R0_TAB_COLBASE[9][9] = " + cbt + ";\n")
+    out.append("__constant__ int c_img_colbase[9][9] = " + cbt + ";\n")
+    out.append("__constant__ unsigned char c_r0_lane[8][256][4] = {\n" + ",\n".join(lane_rows) + "};\n")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "r0_tables.inc")
+    with open(path, "w") as f:
+        f.write("".join(out))
+    print(path)
+
+
+if __name__ == "__main__":
+    main()

@@ -34,9 +34,9 @@ def test_noalloc_matches_score_on_two_calls_in_a_row():
 
 
 def test_noalloc_size_limit_is_an_error():
-    s1, s2 = W.pair(64, 64, 13)  # 8*T(64)*64^2 bytes > 64 MiB
+    s1, s2 = W.pair(115, 64, 13)  # T(115)*10080 bytes of tables + S1 + job lists > 64 MiB
     with pytest.raises(api.BpmaxError) as e:
         api.score_noalloc(s1, s2, W.INTEGER_WEIGHTS)
     assert e.value.status == 1
-    s1, s2 = W.pair(63, 64, 14)  # the largest M that fits at N=64
+    s1, s2 = W.pair(114, 64, 14)  # the largest M that fits at N=64
     assert api.score_noalloc(s1, s2, W.INTEGER_WEIGHTS) > 0
