@@ -36,6 +36,26 @@ constexpr int MAX_NP = 4096;
 // inner table width of a strand-2 length: multiples of 8 up to 64, then multiples of 64
 int padded_width(int N) { return N <= MAX_SMALL_NP ? std::max(8, (N + 7) / 8 * 8) : (N + 63) / 64 * 64; }
 
+// Offset pairs per product job on a diagonal with `cells` cells of P2 offset pairs each, for
+// `resident` CTAs that each take every resident-th job. The launch lasts about
+// ceil(jobs / resident) job lengths, a job of q pairs being 2q items plus one merge
+// (`merge_items` items' worth): pick the chunk count that minimises that.
+long long r0_pairs_per_job(long long cells, long long P2, long long resident, long long qmin, long long qmax,
+                           long long merge_items)
+{
+    long long best_q = std::max(qmin, std::min(qmax, P2)), best_cost = -1;
+    for (long long nch = 1; nch <= std::min<long long>(P2, 64); ++nch) {
+        const long long q = std::max(qmin, std::min(qmax, (P2 + nch - 1) / nch));
+        const long long jobs = cells * ((P2 + q - 1) / q);
+        const long long cost = (jobs + resident - 1) / resident * (2 * q + merge_items);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best_q = q;
+        }
+    }
+    return best_q;
+}
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -70,6 +90,7 @@ struct bpmax_ctx {
     DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
     int r0_occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class NB
     int r0_pairs_per_job = 1 << 20;                 // upper bound of k1 offset pairs per product job
+    int r0_merge_items = 2;                         // cost of one job merge, in items, for job sizing
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -185,9 +206,8 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 const int NB = np / 8, G = R0_TAB_ITEMS[NB];
                 const long long P2 = (d + 1) / 2;  // offset pairs per cell
                 const long long resident = (long long)std::max(1, ctx->r0_occ[NB]) * ctx->sms;
-                // about two jobs per resident CTA: each job ends with one merge of the cell's tile
                 const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(ctx->r0_pairs_per_job, qmin);
-                const long long q = std::max(qmin, std::min(qmax, (cells * P2 + 2 * resident - 1) / (2 * resident)));
+                const long long q = r0_pairs_per_job(cells, P2, resident, qmin, qmax, ctx->r0_merge_items);
                 Plan::Launch rl{d, np, (int)P.r0_jobs.size(), 0};
                 for (long long c0 = 0; c0 < P2; c0 += q)
                     for (int p = 0; p < n; ++p)
@@ -966,7 +986,7 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
         int n_r0 = 0;
         if (d > 0) {
             const long long P2 = (d + 1) / 2;
-            const long long q = std::max<long long>(qmin, (cells * P2 + 2 * resident - 1) / (2 * resident));
+            const long long q = r0_pairs_per_job(cells, P2, resident, qmin, 1 << 20, 2);
             n_r0 = (int)(cells * ((P2 + q - 1) / q));
             noalloc_r0_jobs_kernel<<<(n_r0 + 255) / 256, 256, 0, s>>>(rj, cells, d, (int)q, n_r0);
         }

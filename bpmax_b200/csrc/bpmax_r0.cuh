@@ -21,7 +21,8 @@
 // which is exactly row 8kb+8 of B below the block diagonal and, in the last column, the guard row
 // B[Np]); the R3 row B[8bi] is row 0 of block bi of column bj. The column pads and the lane ->
 // task table (r0_tables.inc) make every quarter-warp's 128-bit loads hit distinct bank groups.
-// Stages form a ring; one CTA barrier per iteration frees the stage the next copies overwrite.
+// Stages form a ring without CTA barriers: each warp counts itself done with a stage (shared
+// atomic) and the last one refills it with the iteration S ahead.
 // Both operands are whole images of the same F tables, so the two uses of a table on one
 // diagonal (as A of cell (a, a+d) and as B of cell (b-d, b)) can meet in L2: jobs visit k1
 // offsets in pairs (w, d-1-w), the offset pair p = min(w, d-1-w) being the same for both uses,
@@ -76,7 +77,9 @@ struct R0Cfg {
     static constexpr int OFF_RED = STAGES * STAGE_BYTES;
     static constexpr int OFF_DST = OFF_RED + 4 * RED_WORDS;
     static constexpr int OFF_BAR = (OFF_DST + 4 * NBLK + 15) / 16 * 16;
-    static constexpr size_t SMEM = (size_t)OFF_BAR + 8 * STAGES;
+    static constexpr int OFF_CNT = OFF_BAR + 8 * STAGES;  // per stage: warps done with it
+    static constexpr size_t SMEM = (size_t)OFF_CNT + 4 * STAGES;
+    static constexpr int WARPS = THREADS / 32;
     static_assert(STAGE_BYTES % 16 == 0 && OFF_RED % 16 == 0 && OFF_BAR % 8 == 0, "shared-memory alignment");
     static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
 };
@@ -127,12 +130,16 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
     int *red_dst = reinterpret_cast<int *>(reinterpret_cast<char *>(smem) + C::OFF_DST);  // float offset of each
                                                                                           // block in a cell image
     uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(smem) + C::OFF_BAR);
+    int *done_cnt = reinterpret_cast<int *>(reinterpret_cast<char *>(smem) + C::OFF_CNT);
     const int tid = threadIdx.x;
     int jid = blockIdx.x;
     if (jid >= njobs) return;
 
     if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(smem_u32(bars + s), 1);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(smem_u32(bars + s), 1);
+            done_cnt[s] = 0;
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int q = tid; q < C::RED_WORDS; q += C::THREADS) red[q] = 0;  // +0: below every partial maximum
@@ -158,20 +165,22 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
     __syncthreads();  // mbarrier init visible
 
     const unsigned smem_base = smem_u32(smem);
-    // announces the bytes of iteration `it` of job `jb` on stage s's mbarrier (thread 0 only; done
-    // before the CTA barrier that precedes the copies, so no copy can complete before it)
+    const int lane = tid & 31;
+    // announces the bytes of iteration `it` of job `jb` on stage s's mbarrier (one thread, before
+    // any copy of that iteration is issued)
     auto expect = [&](int s, const R0Job &jb, int it) {
         const int valid = min(C::G, r0_job_items(jb, d) - it * C::G);
         mbar_arrive_tx(smem_u32(bars + s), (unsigned)(valid * C::ITEM_TX));
     };
-    // issues this thread's copies (whole cell images) of iteration `it` of job `jb` into stage s
-    auto issue = [&](int s, const R0Job &jb, int it) {
+    // issues the copies (whole cell images) of iteration `it` of job `jb` into stage s, spread
+    // over the threads first..first+count-1
+    auto issue = [&](int s, const R0Job &jb, int it, int me, int count) {
         const PairDesc pd = pairs[jb.pair];
         const int M = pd.M, j1 = jb.i1 + d;
         const int valid = min(C::G, r0_job_items(jb, d) - it * C::G);
         const unsigned bar = smem_u32(bars + s);
         const float *Fp = F + pd.F_off;
-        for (int o = tid; o < 2 * valid; o += C::THREADS) {
+        for (int o = me; o < 2 * valid; o += count) {
             const int g = o >> 1, k1 = jb.i1 + r0_item_offset(jb, d, it * C::G + g);
             const long long cell = (o & 1) ? cell_index(M, k1 + 1, j1) : cell_index(M, jb.i1, k1);
             bulk_g2s(smem_base + (unsigned)(s * C::STAGE_BYTES + (g * C::ITEM + (o & 1) * C::IMG) * 16), Fp + cell * CELL,
@@ -179,7 +188,8 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         }
     };
 
-    // consumer position (jid, job, it) and producer position (pj, pjob, pit), S-1 iterations ahead
+    // consumer position (jid, job, it) and producer position (pj, pjob, pit), S iterations ahead;
+    // every warp advances both the same way, so all agree on which iteration each stage holds
     R0Job job = jobs[jid];
     int n_it = (r0_job_items(job, d) + C::G - 1) / C::G, it = 0;
     int pj = jid, pit = 0;
@@ -191,7 +201,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
             if (j_ < njobs) jb_ = jobs[j_];
         }
     };
-    if (tid == 0) {  // expected bytes of the first S-1 iterations and of the first in-loop issue
+    if (tid == 0) {  // expected bytes of the first S iterations (every stage starts free)
         int j_ = pj, it_ = pit;
         R0Job jb_ = pjob;
         for (int s = 0; s < S && j_ < njobs; ++s) {
@@ -201,9 +211,9 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
     }
     __syncthreads();
 #pragma unroll 1
-    for (int s = 0; s < S - 1; ++s)
+    for (int s = 0; s < S; ++s)
         if (pj < njobs) {
-            issue(s, pjob, pit);
+            issue(s, pjob, pit, tid, C::THREADS);
             advance(pj, pjob, pit);
         }
 
@@ -215,23 +225,16 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
 
     unsigned phase = 0;  // bit s: parity of stage s's next completion
     int stage = 0;
-    bool bad = false;
+    bool bad = false;    // an mbarrier wait ran out: skip waits and work, leave at the next job end
 #pragma unroll 1
     while (true) {
-        // every thread is done with the previous iteration: its stage may be refilled
-        if (__syncthreads_or(bad)) return;
-        if (pj < njobs) {
-            issue((stage + S - 1) % S, pjob, pit);
-            advance(pj, pjob, pit);
-        }
         const bool active = has_task && it * C::G + tg < r0_job_items(job, d);
-        if (!mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u)) {
+        if (!bad && !mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u)) {
             atomicExch(err, 1);
             bad = true;
-            continue;  // leave together at the next CTA barrier
         }
         phase ^= 1u << stage;
-        if (active) {
+        if (active && !bad) {
             const float *item = smem + (size_t)stage * C::STAGE * 4 + tg * C::ITEM * 4;
             const float *As = item + a_off, *Bs = item + b_off;
 #pragma unroll
@@ -272,9 +275,22 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
                 for (int j = 0; j < 8; ++j) acc[0][j] = fmaxf(acc[0][j], s1a + rv[j]);
             }
         }
-        // bytes of the next iteration's copies, which refill this stage (thread 0 has finished
-        // waiting on its current phase; the copies start only after the next CTA barrier)
-        if (tid == 0 && pj < njobs) expect(stage, pjob, pit);
+        // the last warp done with this stage refills it with the iteration S ahead
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(done_cnt + stage, 1) == C::WARPS - 1;
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && pj < njobs) {
+            if (lane == 0) {
+                done_cnt[stage] = 0;
+                expect(stage, pjob, pit);
+            }
+            __syncwarp();
+            issue(stage, pjob, pit, lane, 32);
+        } else if (last && lane == 0) {
+            done_cnt[stage] = 0;
+        }
+        if (pj < njobs) advance(pj, pjob, pit);
         if (++it >= n_it) {  // job done: merge the partial maxima of all tasks into F(i1, i1+d)
             const PairDesc pd = pairs[job.pair];
             if (has_task) {
@@ -288,7 +304,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
                         acc[i][j] = NEG_INF;
                     }
             }
-            __syncthreads();
+            if (__syncthreads_or(bad)) return;
             int *out = reinterpret_cast<int *>(F + pd.F_off + cell_index(pd.M, job.i1, job.i1 + d) * CELL);
             for (int e = tid; e < 64 * C::NBLK; e += C::THREADS) {
                 const int q = e >> 6, w = e & 63;
@@ -298,6 +314,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
                     red[65 * q + w] = 0;
                 }
             }
+            __syncthreads();  // the tile is clear before any warp merges its next job into it
             jid += gridDim.x;
             if (jid >= njobs) break;
             job = jobs[jid];
