@@ -31,6 +31,7 @@ using namespace bpmax;
 namespace {
 
 constexpr int MAX_SMALL_NP = 64;
+constexpr int MAX_CLASS_STREAMS = 8;  // side streams for the per-width-class chains of a batch
 constexpr int MAX_NP = 4096;
 
 // inner table width of a strand-2 length: multiples of 8 up to 64, then multiples of 64
@@ -74,6 +75,7 @@ struct Plan {
     std::vector<R0Job> r0_jobs;
     std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > 64 (first/count index this array)
     std::vector<CellJob> cell_jobs;
+    std::vector<int> classes;  // distinct inner widths, ascending
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
 };
@@ -84,6 +86,8 @@ struct bpmax_ctx {
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t class_stream[8] = {};  // MAX_CLASS_STREAMS
+    cudaEvent_t fork_ev = nullptr, join_ev[8] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
     std::string err;
@@ -164,12 +168,10 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         s = align64(s + (long long)Ms[p] * Ms[p]);
         pd.S2_off = s;
         s = align64(s + (long long)pd.Np * pd.Np);
-        if (pd.Np > MAX_SMALL_NP) {
-            pd.S2m_off = s;
-            s = align64(s + (long long)pd.Np * pd.Np);
-            pd.S2t_off = s;
-            s = align64(s + (long long)pd.Np * pd.Np);
-        }
+        pd.S2m_off = s;  // masked copies of S2 read by the inner wavefront
+        s = align64(s + (long long)pd.Np * pd.Np);
+        pd.S2t_off = s;
+        s = align64(s + (long long)pd.Np * pd.Np);
         pd.seq1_off = b;
         b += Ms[p];
         pd.seq2_off = b;
@@ -184,6 +186,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     for (const auto &pd : P.pairs) classes.push_back(pd.Np);
     std::sort(classes.begin(), classes.end());
     classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
+    P.classes = classes;
     // jobs, grouped by diagonal then inner width class
     const int target = 4 * ctx->sms;  // CTAs per diagonal launch worth splitting k1 for (wide tables)
     for (int d = 0; d < P.maxM; ++d) {
@@ -244,37 +247,37 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     return BPMAX_OK;
 }
 
-void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L)
+void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
     const int grid = std::min(L.count, 3 * ctx->sms);
-    r0_large_kernel<<<grid, 128, WideShape::SMEM, ctx->stream>>>(
+    r0_large_kernel<<<grid, 128, WideShape::SMEM, s>>>(
         (const R0JobL *)ctx->r0ljobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p,
         (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
 }
 
-void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L)
+void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
     constexpr int W = FIN_LARGE_THREADS / 32;
-    finalize_large_kernel<<<L.count + (L.s1_count + W - 1) / W, FIN_LARGE_THREADS, 0, ctx->stream>>>(
+    finalize_large_kernel<<<L.count + (L.s1_count + W - 1) / W, FIN_LARGE_THREADS, 0, s>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
         (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
         (const uint8_t *)ctx->bases.p, ctx->W, L.d);
 }
 
 template <int NB>
-void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L)
+void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
     using C = R0Cfg<NB>;
     const int grid = std::min(L.count, std::max(1, ctx->r0_occ[NB]) * ctx->sms);  // resident CTAs; each loops over jobs
-    r0_kernel<NB><<<grid, C::THREADS, C::SMEM, ctx->stream>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
+    r0_kernel<NB><<<grid, C::THREADS, C::SMEM, s>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
                                                               (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
                                                               (int *)ctx->errflag.p);
 }
 
 template <int NB>
-void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L)
+void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
-    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, FinShape<8 * NB>::SMEM, ctx->stream>>>(
+    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, FinShape<8 * NB>::SMEM, s>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
         (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W,
         L.d);
@@ -334,38 +337,58 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         s2_aux_kernel<<<(int)P.pairs.size(), 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (float *)ctx->S.p);
     }
     launches += 2;
+    // pairs of different inner widths never interact: each width class runs its own chain of
+    // diagonals on its own stream (parallel branches of the captured graph); profiling runs
+    // serialise everything on the main stream so every launch can be timed
+    const bool fork = !(kp && kp->on) && P.classes.size() > 1;
+    auto stream_of = [&](int np) {
+        if (!fork) return ctx->stream;
+        const int k = (int)(std::find(P.classes.begin(), P.classes.end(), np) - P.classes.begin());
+        return ctx->class_stream[k % MAX_CLASS_STREAMS];
+    };
+    const int nstreams = fork ? std::min((int)P.classes.size(), MAX_CLASS_STREAMS) : 0;
+    if (fork) {
+        CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+        for (int k = 0; k < nstreams; ++k) CK(cudaStreamWaitEvent(ctx->class_stream[k], ctx->fork_ev, 0));
+    }
     size_t ri = 0, fi = 0;
     for (int d = 0; d < P.maxM; ++d) {
         for (; ri < P.r0_launches.size() && P.r0_launches[ri].d == d; ++ri, ++launches) {
             const auto &L = P.r0_launches[ri];
+            const cudaStream_t st = stream_of(L.np);
             ProfScope ps(ctx, kp, 1);
             switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-            case 0: launch_r0_large(ctx, L); break;
-            case 1: launch_r0<1>(ctx, L); break;
-            case 2: launch_r0<2>(ctx, L); break;
-            case 3: launch_r0<3>(ctx, L); break;
-            case 4: launch_r0<4>(ctx, L); break;
-            case 5: launch_r0<5>(ctx, L); break;
-            case 6: launch_r0<6>(ctx, L); break;
-            case 7: launch_r0<7>(ctx, L); break;
-            default: launch_r0<8>(ctx, L); break;
+            case 0: launch_r0_large(ctx, L, st); break;
+            case 1: launch_r0<1>(ctx, L, st); break;
+            case 2: launch_r0<2>(ctx, L, st); break;
+            case 3: launch_r0<3>(ctx, L, st); break;
+            case 4: launch_r0<4>(ctx, L, st); break;
+            case 5: launch_r0<5>(ctx, L, st); break;
+            case 6: launch_r0<6>(ctx, L, st); break;
+            case 7: launch_r0<7>(ctx, L, st); break;
+            default: launch_r0<8>(ctx, L, st); break;
             }
         }
         for (; fi < P.fin_launches.size() && P.fin_launches[fi].d == d; ++fi, ++launches) {
             const auto &L = P.fin_launches[fi];
+            const cudaStream_t st = stream_of(L.np);
             ProfScope ps(ctx, kp, 2);
             switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-            case 0: launch_fin_large(ctx, L); break;
-            case 1: launch_fin<1>(ctx, L); break;
-            case 2: launch_fin<2>(ctx, L); break;
-            case 3: launch_fin<3>(ctx, L); break;
-            case 4: launch_fin<4>(ctx, L); break;
-            case 5: launch_fin<5>(ctx, L); break;
-            case 6: launch_fin<6>(ctx, L); break;
-            case 7: launch_fin<7>(ctx, L); break;
-            default: launch_fin<8>(ctx, L); break;
+            case 0: launch_fin_large(ctx, L, st); break;
+            case 1: launch_fin<1>(ctx, L, st); break;
+            case 2: launch_fin<2>(ctx, L, st); break;
+            case 3: launch_fin<3>(ctx, L, st); break;
+            case 4: launch_fin<4>(ctx, L, st); break;
+            case 5: launch_fin<5>(ctx, L, st); break;
+            case 6: launch_fin<6>(ctx, L, st); break;
+            case 7: launch_fin<7>(ctx, L, st); break;
+            default: launch_fin<8>(ctx, L, st); break;
             }
         }
+    }
+    for (int k = 0; k < nstreams; ++k) {  // join the class chains back into the main stream
+        CK(cudaEventRecord(ctx->join_ev[k], ctx->class_stream[k]));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev[k], 0));
     }
     CK(cudaGetLastError());
     P.launches = launches;
@@ -549,8 +572,13 @@ int bpmax_gpu_create(int device, bpmax_ctx **out)
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->stage_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->stage_ev[1], cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&ctx->stage_ev[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess)
         st = BPMAX_ECUDA;
+    for (int k = 0; k < MAX_CLASS_STREAMS && st == BPMAX_OK; ++k)
+        if (cudaStreamCreateWithFlags(&ctx->class_stream[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
+            st = BPMAX_ECUDA;
     if (st == BPMAX_OK) st = set_smem_attr<1>(ctx);
     if (st == BPMAX_OK) st = set_smem_attr<2>(ctx);
     if (st == BPMAX_OK) st = set_smem_attr<3>(ctx);
@@ -583,6 +611,11 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    for (int k = 0; k < MAX_CLASS_STREAMS; ++k) {
+        if (ctx->class_stream[k]) cudaStreamDestroy(ctx->class_stream[k]);
+        if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -925,7 +958,8 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     const long long nF = (long long)M * (M + 1) / 2 * cell_floats(Np);
     const long long off_S = align64(nF);
     const long long S2_rel = align64((long long)M * M);
-    const long long off_seq = off_S + align64(S2_rel + (long long)Np * Np);
+    const long long S2m_rel = S2_rel + align64((long long)Np * Np), S2t_rel = S2m_rel + align64((long long)Np * Np);
+    const long long off_seq = off_S + S2t_rel + align64((long long)Np * Np);
     const long long off_bases = off_seq + align64(M + N);
     const long long off_pd = off_bases + align64((M + N + 3) / 4);
     const long long off_score = off_pd + align64((long long)(sizeof(PairDesc) + 3) / 4);  // score, error flag
@@ -963,6 +997,8 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     pd.F_off = 0;
     pd.S1_off = 0;
     pd.S2_off = S2_rel;
+    pd.S2m_off = S2m_rel;
+    pd.S2t_off = S2t_rel;
     pd.seq1_off = 0;
     pd.seq2_off = (int)M;
     Weights W;
@@ -981,6 +1017,7 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     }
     noalloc_prep_kernel<<<8, 256, 0, s>>>(seqs, (int)M, (int)N, bases, cj);
     single_strand_kernel<<<1, 512, 0, s>>>(pdp, bases, S, W);
+    s2_aux_kernel<<<1, 256, 0, s>>>(pdp, S);
     for (int d = 0; d < (int)M; ++d) {
         const int cells = (int)M - d;
         int n_r0 = 0;

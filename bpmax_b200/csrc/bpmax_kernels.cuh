@@ -187,6 +187,9 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     constexpr long long CELL = 4LL * R0_TAB_COLBASE[NB][NB];
     extern __shared__ __align__(16) float fsm[];
     __shared__ int cbs[NB];  // float offset of each block column in the cell image
+    __shared__ float wsh[12];  // the weight table (indexed by pair type)
+    if (threadIdx.x < 12) wsh[threadIdx.x] = W.w[threadIdx.x];
+    __syncthreads();
     float *Fs = fsm, *FT1 = fsm + Sh::TBL, *Ss = fsm + 2 * Sh::TBL, *ST1 = fsm + 3 * Sh::TBL;
     uint8_t *sb = reinterpret_cast<uint8_t *>(fsm + 4 * Sh::TBL);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -208,7 +211,7 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
         if (k < j) r0 = fmaxf(r0, S1[i * M + k] + S1[(k + 1) * M + j]);
         float red = fmaxf(r0, r1);
         for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
-        if (lane == 0) S1[i * M + j] = fmaxf(S1[(i + 1) * M + (j - 1)] + score_w(W.w, s1[i], s1[j]), red);
+        if (lane == 0) S1[i * M + j] = fmaxf(S1[(i + 1) * M + (j - 1)] + score_w(wsh, s1[i], s1[j]), red);
         return;
     }
     const CellJob job = jobs[blockIdx.x];
@@ -241,7 +244,7 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
             const bool valid = r <= c && c < N;
             sv[e] = valid ? bv[e] : NEG_INF;
             float v = NEG_INF;
-            if (valid) v = (d == 0 && r == c) ? score_w(W.w + 6, s1[i1], sb[r]) : fmaxf(av[e], s1v + bv[e]);
+            if (valid) v = (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(av[e], s1v + bv[e]);
             fv[e] = v;
             if (r >= 1) { FT1[c * LD + r - 1] = v; ST1[c * LD + r - 1] = sv[e]; }
         }
@@ -275,7 +278,7 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
         for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
         if (act && lane_g == 0) {
             float v = fmaxf(Fs[i2 * LD + j2], red);
-            if (dd >= 4) v = fmaxf(v, Fs[(i2 + 1) * LD + (j2 - 1)] + score_w(W.w, sb[i2], sb[j2]));
+            if (dd >= 4) v = fmaxf(v, Fs[(i2 + 1) * LD + (j2 - 1)] + score_w(wsh, sb[i2], sb[j2]));
             Fs[i2 * LD + j2] = v;
             if (i2 >= 1) FT1[j2 * LD + i2 - 1] = v;
         }
@@ -284,7 +287,7 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     // write-back, 4 columns of one block row per step; SW1 candidate of cell (i1-1, j1+1), whose
     // table nothing else has written yet
     const bool push = i1 >= 1 && j1 + 1 < M && d + 2 >= 4;
-    const float wp = push ? score_w(W.w, s1[i1 - 1], s1[j1 + 1]) : 0.0f;
+    const float wp = push ? score_w(wsh, s1[i1 - 1], s1[j1 + 1]) : 0.0f;
     float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * CELL : nullptr;
     for (int q4 = tid; q4 < NBLK * 16; q4 += 128) {
         int BI, BJ;

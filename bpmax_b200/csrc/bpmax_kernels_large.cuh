@@ -60,14 +60,13 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 
 // ------------------------------------------------------------------------------------------
-// Masked copies of S2 for the large finalize: S2M[i][k] = S2(i,k) if i <= k < N else -inf and
+// Masked copies of S2: S2M[i][k] = S2(i,k) if i <= k < N else -inf and
 // ST1[j][k] = S2(k+1,j) if k+1 <= j < N else -inf (S2 over the reversed strand 2,
-// V3/bpmax_verify.c:560-571). One CTA per pair; pairs with Np <= 64 are skipped.
+// V3/bpmax_verify.c:560-571), read by the inner wavefront of every width. One CTA per pair.
 // ------------------------------------------------------------------------------------------
 __global__ void s2_aux_kernel(const PairDesc *__restrict__ pairs, float *__restrict__ S)
 {
     const PairDesc pd = pairs[blockIdx.x];
-    if (pd.Np <= 64) return;
     const int Np = pd.Np, N = pd.N;
     const float *S2 = S + pd.S2_off;
     float *S2M = S + pd.S2m_off, *ST1 = S + pd.S2t_off;
