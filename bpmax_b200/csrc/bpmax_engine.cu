@@ -277,7 +277,8 @@ void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 template <int NB>
 void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
-    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + 3) / 4, 128, FinShape<8 * NB>::SMEM, s>>>(
+    using Sh = FinShape<8 * NB>;
+    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
         (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W,
         L.d);
@@ -936,7 +937,8 @@ void noalloc_launch_diag(cudaStream_t s, const NoallocDevice &nd, int d, int n_r
         r0_kernel<NB><<<std::min(n_r0, std::max(1, nd.occ[NB]) * nd.sms), R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM, s>>>(
             rj, n_r0, pd, F, d, err);
     const int n_s1 = n_cells - 1;  // S1 cells of diagonal d+1: the first n_cells-1 entries of cj
-    finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + 3) / 4, 128, FinShape<8 * NB>::SMEM, s>>>(
+    using Sh = FinShape<8 * NB>;
+    finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
         cj, n_cells, cj, n_s1, pd, F, S, bases, W, d);
 }
 

@@ -137,9 +137,8 @@ __global__ void single_strand_kernel(const PairDesc *__restrict__ pairs, const u
 }
 
 // ------------------------------------------------------------------------------------------
-// Finalize the outer cells of diagonal d (Np = 8*NB <= 64, cell images; 4 warps per cell):
-// adds the candidates that do not come from R0/R3/R4 and runs the inner wavefront of R1/R2/SW2 in
-// shared memory.
+// Finalize the outer cells of diagonal d (Np <= 64, cell images; one CTA per cell):
+// adds the candidates that do not come from R0/R3/R4 and runs the inner wavefront of R1/R2/SW2.
 //   base  i1==j1 && i2==j2: inter(s1[i1], s2r[i2])            (assignment, eval_FTable :576)
 //   S1(i1,j1)+S2(i2,j2)
 //   SW2 = F(i1,j1,i2+1,j2-1)+intra(s2r[i2],s2r[j2]) if j2-i2>=4
@@ -149,6 +148,14 @@ __global__ void single_strand_kernel(const PairDesc *__restrict__ pairs, const u
 // finalize of (i1+1, j1-1) two diagonals earlier, before any product touched it. Every literal-0
 // candidate is covered because every value is >= +0. Writes the cell's blocks (-inf outside the
 // logical triangle, S1(i1,j1) on the subdiagonal) and its S1 pieces.
+// The inner wavefront pushes forward: every inner cell (i2,j2), e2 = j2-i2 >= 1, has one owner
+// thread that keeps its running maximum in a register. When inner diagonal e is final, each
+// owner adds its two candidates that read diagonal e,
+//   R1 with k2 = i2+e:    F[i2][i2+e] + S2(i2+e+1, j2)
+//   R2 with k2 = j2-e-1:  S2(i2, j2-e-1) + F[j2-e][j2]
+// to every open cell (e2 > e); the cells of diagonal e+1 have then seen all their R1/R2 terms
+// and are final after SW2. One CTA barrier per inner diagonal; the diagonals are kept in shared
+// memory diagonal-major, D[e][i2] = F[i2][i2+e].
 // CTAs after the first njobs compute S1 on diagonal d+1 (V3/bpmax_verify.c:533-544), one warp
 // per cell, from S1 diagonals <= d (S1 is cleared to 0 before the fill; j-i <= 3 stays 0).
 // ------------------------------------------------------------------------------------------
@@ -158,12 +165,14 @@ struct CellJob {
 
 template <int NP>
 struct FinShape {
-    static constexpr int LD = NP + 4;             // 16-byte rows; conflict-free column walks
-    static constexpr int TBL = NP * LD;           // one NP x NP table
-    static constexpr size_t SMEM = 4 * (size_t)TBL * sizeof(float) + NP;
+    // threads per cell: the wavefront's serial work per step is K owned cells per thread
+    static constexpr int THREADS = NP >= 48 ? 512 : (NP >= 24 ? 256 : 128);
+    static constexpr int WARPS = THREADS / 32;
+    static constexpr int K = (NP * (NP - 1) / 2 + THREADS - 1) / THREADS;  // owned inner cells per thread
+    static constexpr size_t SMEM = 2 * (size_t)NP * NP * sizeof(float) + NP;  // D, S2, bases
 };
 
-// (BI, BJ) of the q-th block of a block-packed table (row-major triangle order)
+// (BI, BJ) of the q-th block of the upper block triangle (row-major triangle order)
 __device__ __forceinline__ void blk_decode(int NB, int q, int &BI, int &BJ)
 {
     BI = 0;
@@ -171,30 +180,26 @@ __device__ __forceinline__ void blk_decode(int NB, int q, int &BI, int &BJ)
     BJ = BI + q;
 }
 
-// The inner DP reads, for cell (i2,j2):  R1 = max_k F[i2][k] + S2[k+1][j2],  R2 = max_k S2[i2][k] + F[k+1][j2].
-// Shared memory keeps F and S2 row-major plus shifted transposes FT1[j2][k] = F[k+1][j2] and
-// ST1[j2][k] = S2[k+1][j2], so both are row-by-row scans with 16-byte loads. Every entry outside
-// the logical triangles is -inf, so 4-aligned k chunks that overhang [i2, j2) only add -inf terms
-// (k < i2 meets F[i2][k] or S2[i2][k]; k >= j2 meets ST1[j2][k] or FT1[j2][k]).
 template <int NP>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(FinShape<NP>::THREADS)
 finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
                       const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ S,
                       const uint8_t *__restrict__ bases, Weights W, int d)
 {
     using Sh = FinShape<NP>;
-    constexpr int LD = Sh::LD, NB = NP / 8, NBLK = NB * (NB + 1) / 2;
+    constexpr int NB = NP / 8, NBLK = NB * (NB + 1) / 2, K = Sh::K;
     constexpr long long CELL = 4LL * R0_TAB_COLBASE[NB][NB];
     extern __shared__ __align__(16) float fsm[];
-    __shared__ int cbs[NB];  // float offset of each block column in the cell image
+    float *D = fsm, *S2s = fsm + NP * NP;
+    uint8_t *sb = reinterpret_cast<uint8_t *>(fsm + 2 * NP * NP);
+    __shared__ int cbs[NB];    // float offset of each block column in the cell image
     __shared__ float wsh[12];  // the weight table (indexed by pair type)
-    if (threadIdx.x < 12) wsh[threadIdx.x] = W.w[threadIdx.x];
-    __syncthreads();
-    float *Fs = fsm, *FT1 = fsm + Sh::TBL, *Ss = fsm + 2 * Sh::TBL, *ST1 = fsm + 3 * Sh::TBL;
-    uint8_t *sb = reinterpret_cast<uint8_t *>(fsm + 4 * Sh::TBL);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < 12) wsh[tid] = W.w[tid];
+    if (tid < NB) cbs[tid] = 4 * c_img_colbase[NB][tid];
+    __syncthreads();
     if ((int)blockIdx.x >= njobs) {  // S1 cells (i, i+d+1), one per warp
-        const int q = ((int)blockIdx.x - njobs) * 4 + warp;
+        const int q = ((int)blockIdx.x - njobs) * Sh::WARPS + warp;
         if (q >= ns1) return;
         const CellJob job = s1jobs[q];
         const PairDesc pd = pairs[job.pair];
@@ -223,64 +228,48 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     const uint8_t *s1 = bases + pd.seq1_off;
     const uint8_t *s2r = bases + pd.seq2_off;
     const float s1v = S1[i1 * M + j1];
-    for (int q = tid; q < NP; q += 128) sb[q] = q < N ? s2r[q] : 4;
-    if (tid < NB) cbs[tid] = 4 * c_img_colbase[NB][tid];
-    __syncthreads();  // sb and cbs are read by the staging loop
-    // staging, 4 consecutive columns per step: the accumulated F (max of R0, R3, R4, SW1; blocks
-    // below the block diagonal are not stored) and S2
-    for (int q4 = tid; q4 < NP * NP / 4; q4 += 128) {
-        const int r = (4 * q4) / NP, c0 = (4 * q4) % NP;
-        float av[4] = {NEG_INF, NEG_INF, NEG_INF, NEG_INF};
-        if ((r >> 3) <= (c0 >> 3)) {
-            const float4 a = *reinterpret_cast<const float4 *>(Fc + cbs[c0 >> 3] + 68 * (r >> 3) + 8 * (r & 7) + (c0 & 7));
-            av[0] = a.x; av[1] = a.y; av[2] = a.z; av[3] = a.w;
-        }
-        const float4 b = *reinterpret_cast<const float4 *>(S2 + 4 * q4);
-        const float bv[4] = {b.x, b.y, b.z, b.w};
-        float fv[4], sv[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int c = c0 + e;
-            const bool valid = r <= c && c < N;
-            sv[e] = valid ? bv[e] : NEG_INF;
-            float v = NEG_INF;
-            if (valid) v = (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(av[e], s1v + bv[e]);
-            fv[e] = v;
-            if (r >= 1) { FT1[c * LD + r - 1] = v; ST1[c * LD + r - 1] = sv[e]; }
-        }
-        *reinterpret_cast<float4 *>(Fs + r * LD + c0) = make_float4(fv[0], fv[1], fv[2], fv[3]);
-        *reinterpret_cast<float4 *>(Ss + r * LD + c0) = make_float4(sv[0], sv[1], sv[2], sv[3]);
-    }
-    for (int c = tid; c < NP; c += 128) { FT1[c * LD + NP - 1] = NEG_INF; ST1[c * LD + NP - 1] = NEG_INF; }
+    for (int q4 = tid; q4 < NP * NP / 4; q4 += Sh::THREADS)
+        *reinterpret_cast<float4 *>(S2s + 4 * q4) = *reinterpret_cast<const float4 *>(S2 + 4 * q4);
+    for (int q = tid; q < NP; q += Sh::THREADS) sb[q] = q < N ? s2r[q] : 4;
     __syncthreads();
-    for (int dd = 1; dd < N; ++dd) {
-        const int cells = N - dd;  // <= 63 < 128: one pass
-        const int g = min(32, 1 << (31 - __clz(128 / cells)));
-        const int lane_g = tid & (g - 1);
-        const int i2 = tid / g, j2 = i2 + dd;
-        const bool act = i2 < cells;
-        float r0 = NEG_INF, r1 = NEG_INF;
-        if (act) {
-            const float *fr = Fs + i2 * LD, *sr = Ss + i2 * LD, *ftr = FT1 + j2 * LD, *str = ST1 + j2 * LD;
-            const int c_end = (j2 + 3) >> 2;
-            for (int c = (i2 >> 2) + lane_g; c < c_end; c += g) {
-                const float4 f = *reinterpret_cast<const float4 *>(fr + 4 * c);
-                const float4 t = *reinterpret_cast<const float4 *>(str + 4 * c);
-                const float4 s2 = *reinterpret_cast<const float4 *>(sr + 4 * c);
-                const float4 u = *reinterpret_cast<const float4 *>(ftr + 4 * c);
-                r0 = fmax3(r0, f.x + t.x, s2.x + u.x);
-                r1 = fmax3(r1, f.y + t.y, s2.y + u.y);
-                r0 = fmax3(r0, f.z + t.z, s2.z + u.z);
-                r1 = fmax3(r1, f.w + t.w, s2.w + u.w);
-            }
+    // accumulated value of inner cell (r, c), r <= c, from the cell image
+    auto img = [&](int r, int c) { return Fc[cbs[c >> 3] + 68 * (r >> 3) + 8 * (r & 7) + (c & 7)]; };
+    // owned inner cells c = tid + THREADS*k among the N(N-1)/2 cells with e2 >= 1, ordered by
+    // (e2, i2): running maxima start at max(accumulated, S1+S2)
+    const int ncells = N * (N - 1) / 2;
+    int cell_i[K], cell_e[K];
+    float acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const int c = tid + Sh::THREADS * k;
+        cell_e[k] = NP;  // no cell: never open
+        cell_i[k] = 0;
+        acc[k] = NEG_INF;
+        if (c < ncells) {
+            int e = 1, rem = c;
+            while (rem >= N - e) { rem -= N - e; ++e; }
+            cell_e[k] = e;
+            cell_i[k] = rem;
+            acc[k] = fmaxf(img(rem, rem + e), s1v + S2s[rem * NP + rem + e]);
         }
-        float red = fmaxf(r0, r1);
-        for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
-        if (act && lane_g == 0) {
-            float v = fmaxf(Fs[i2 * LD + j2], red);
-            if (dd >= 4) v = fmaxf(v, Fs[(i2 + 1) * LD + (j2 - 1)] + score_w(wsh, sb[i2], sb[j2]));
-            Fs[i2 * LD + j2] = v;
-            if (i2 >= 1) FT1[j2 * LD + i2 - 1] = v;
+    }
+    if (tid < N)  // inner diagonal 0
+        D[tid] = d == 0 ? score_w(wsh + 6, s1[i1], sb[tid]) : fmaxf(img(tid, tid), s1v + S2s[tid * NP + tid]);
+    __syncthreads();
+    for (int e = 0; e + 1 < N; ++e) {
+        const float *De = D + e * NP;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int e2 = cell_e[k];
+            if (e2 > e && e2 < NP) {
+                const int i2 = cell_i[k], j2 = i2 + e2;
+                acc[k] = fmax3(acc[k], De[i2] + S2s[(i2 + e + 1) * NP + j2], S2s[i2 * NP + j2 - e - 1] + De[j2 - e]);
+                if (e2 == e + 1) {  // all R1/R2 terms seen: SW2, then the cell is final
+                    float v = acc[k];
+                    if (e2 >= 4) v = fmaxf(v, D[(e2 - 2) * NP + i2 + 1] + score_w(wsh, sb[i2], sb[j2]));
+                    D[e2 * NP + i2] = v;
+                }
+            }
         }
         __syncthreads();
     }
@@ -289,26 +278,21 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     const bool push = i1 >= 1 && j1 + 1 < M && d + 2 >= 4;
     const float wp = push ? score_w(wsh, s1[i1 - 1], s1[j1 + 1]) : 0.0f;
     float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * CELL : nullptr;
-    for (int q4 = tid; q4 < NBLK * 16; q4 += 128) {
+    for (int q4 = tid; q4 < NBLK * 16; q4 += Sh::THREADS) {
         int BI, BJ;
         blk_decode(NB, q4 >> 4, BI, BJ);
-        const int r = 8 * BI + ((q4 & 15) >> 1), c = 8 * BJ + 4 * (q4 & 1);
-        float4 v = *reinterpret_cast<const float4 *>(Fs + r * LD + c);
-        const int o = cbs[BJ] + 68 * BI + 4 * (q4 & 15);  // block (BI, BJ), row r & 7, half (c & 7) / 4
-        if (push) {
-            float4 u;
-            u.x = (r <= c + 0 && c + 0 < N) ? v.x + wp : 0.0f;
-            u.y = (r <= c + 1 && c + 1 < N) ? v.y + wp : 0.0f;
-            u.z = (r <= c + 2 && c + 2 < N) ? v.z + wp : 0.0f;
-            u.w = (r <= c + 3 && c + 3 < N) ? v.w + wp : 0.0f;
-            *reinterpret_cast<float4 *>(Fn + o) = u;
+        const int r = 8 * BI + ((q4 & 15) >> 1), c0 = 8 * BJ + 4 * (q4 & 1);
+        float v[4], u[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int c = c0 + t;
+            const bool valid = r <= c && c < N;
+            v[t] = valid ? D[(c - r) * NP + r] : (r == c + 1 ? s1v : NEG_INF);  // S1 on the subdiagonal
+            u[t] = valid ? v[t] + wp : 0.0f;
         }
-        // S1(i1,j1) on the subdiagonal (never a logical cell): the R3/R4 slots of the product
-        if (r == c + 1) v.x = s1v;
-        if (r == c + 2) v.y = s1v;
-        if (r == c + 3) v.z = s1v;
-        if (r == c + 4) v.w = s1v;
-        *reinterpret_cast<float4 *>(Fc + o) = v;
+        const int o = cbs[BJ] + 68 * BI + 4 * (q4 & 15);  // block (BI, BJ), row r & 7, half
+        if (push) *reinterpret_cast<float4 *>(Fn + o) = make_float4(u[0], u[1], u[2], u[3]);
+        *reinterpret_cast<float4 *>(Fc + o) = make_float4(v[0], v[1], v[2], v[3]);
     }
     if (tid < 2 * NB) {  // S1 piece of every block column: -inf x7, S1(i1,j1)
         const int BJ = tid >> 1, h = tid & 1;
