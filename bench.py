@@ -277,13 +277,9 @@ def main_b200(args, world, rank, local):
     prof = eng.profile_kernels()
     r0_ms, r0_n, r0_terms = prof["r0"]
     peak = eng.maxplus_peak()
-    achieved = r0_terms / (r0_ms * 1e-3) / 1e9
-    roofline = {"bound": "fp32_alu", "kernel": "r0_small_kernel (R0+R3+R4 max-plus product)",
-                "achieved": achieved, "peak": peak / 1e9, "unit": "Gterms/s", "frac": achieved * 1e9 / peak,
-                "peak_source": "measured live: bpmax_gpu_maxplus_peak (register-resident fp32 add + 3-input max on all SMs)",
-                "r0_launches_per_step": r0_n, "r0_ms_per_step": r0_ms,
-                "r0_share_of_step": r0_ms / sum(v[0] for v in prof.values()), "traffic": None,
-                "kernels": {k: {"ms": v[0], "launches": v[1], "terms": v[2]} for k, v in prof.items()}}
+    roofline = r0_roofline(wl, r0_ms, r0_n, r0_terms, peak, clocks)
+    roofline["kernels"] = {k: {"ms": v[0], "launches": v[1], "terms": v[2]} for k, v in prof.items()}
+    roofline["r0_share_of_step"] = r0_ms / sum(v[0] for v in prof.values())
 
     e2e = None
     if not args.no_e2e and single and len(s2) >= 8:
@@ -312,11 +308,58 @@ def main_b200(args, world, rank, local):
                            "weights": [float(x) for x in wl.weights],
                            "l2": "inputs larger than L2 (each step streams its F tables from HBM)",
                            "parallelism": f"independent pairs per rank x{world}"},
-                "pct_fp32_alu_peak": 100.0 * value * 1e9 / peak,
+                "pct_maxplus_peak": 100.0 * value * 1e9 / peak,
                 "gpu_launches": launches, "wall_s": wall, "clocks": clocks, "roofline": roofline,
                 "cpu_baseline": cpu, "e2e": e2e, "batched": batched}
         print(json.dumps(line))
     eng.close()
+
+
+# DRAM bytes (read + write) per product item (one outer cell and one k1) of the R0 kernel with
+# inner width 64, from one ncu capture of a 512x64 fill (profiles/r0_kernel_512x64.md): the
+# kernel's traffic grows with the items it processes.
+R0_DRAM_BYTES_PER_ITEM_NP64 = 16558
+
+
+def r0_roofline(wl, r0_ms, r0_n, r0_terms, peak_terms_s, clocks):
+    """Roofline of the dominant kernel (the R0+R3+R4 product): FP32-ALU bound. One max-plus term is
+    one fp32 add + one max, counted as 2 FP32 operations as the reference counts its GFLOPS.
+    achieved = algorithmic terms per launch / mean launch time (CUDA events on the launching stream).
+    peak = the max-plus issue ceiling measured live on this GPU (register-resident add + 3-input max
+    on every SM). Also reported: the nominal FP32-lane peak (148 SMs x 128 lanes x SM clock, 2 ops
+    per term) and the HBM side of the same kernel (ncu DRAM bytes per launch vs measured copy peak)."""
+    per_launch_s = r0_ms * 1e-3 / max(r0_n, 1)
+    terms_per_launch = r0_terms / max(r0_n, 1)
+    achieved = 2 * terms_per_launch / per_launch_s / 1e12  # TFLOP/s
+    peak = 2 * peak_terms_s / 1e12
+    out = {"bound": "fp32_alu", "kernel": "r0_kernel (R0+R3+R4 max-plus product)", "achieved": achieved, "peak": peak,
+           "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+           "peak_source": "measured live: bpmax_gpu_maxplus_peak (fp32 add + 3-input max, register resident, all SMs)",
+           "ops_per_term": 2, "achieved_Gterms_s": achieved / 2 * 1e3, "launches": r0_n,
+           "ms_per_launch": per_launch_s * 1e3, "terms_per_launch": terms_per_launch}
+    mhz = clocks.get("sm_mhz") or 1965.0
+    nominal = 148 * 128 * mhz * 1e6 / 1e12  # FP32 lane-ops/s in T
+    out["nominal_fp32_peak"] = nominal
+    out["frac_of_nominal_fp32"] = achieved / nominal
+    if R0_DRAM_BYTES_PER_ITEM_NP64 and len(wl.pairs) == 1 and len(wl.pairs[0][1]) > 56 and len(wl.pairs[0][1]) <= 64:
+        M = len(wl.pairs[0][0])
+        items_per_launch = (M * (M * M - 1) / 6) / max(r0_n, 1)
+        traffic = R0_DRAM_BYTES_PER_ITEM_NP64 * items_per_launch
+        out["traffic"] = traffic
+        hbm = measured_peaks().get("hbm_gbs")
+        gbs = traffic / per_launch_s / 1e9
+        out["hbm"] = {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if hbm else None,
+                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per item, scaled to a launch"}
+    return out
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 def measure_e2e(eng, wl, args, world):

@@ -472,7 +472,7 @@ int run_fill(bpmax_ctx *ctx)
     CK(cudaEventSynchronize(ctx->ev1));
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
-    ctx->last_launches = P.launches;
+    ctx->last_launches = P.launches + 1;  // + the score gather
     if (errv) return fail(ctx, BPMAX_ETIMEOUT, "a product kernel gave up waiting for its operand copies");
     return BPMAX_OK;
 }
