@@ -130,22 +130,24 @@ def dist_setup(args):
     return world, rank, local
 
 
-def barrier(world):
+def barrier(world, device: str = "cuda"):
     if world > 1:
         import torch
         import torch.distributed as dist
 
         dist.barrier()
-        torch.cuda.synchronize()
+        if device == "cuda":
+            torch.cuda.synchronize()
 
 
-def reduce_max(world, x: float) -> float:
+def reduce_max(world, x: float, device: str = "cuda") -> float:
+    """The max over ranks of x (one all-reduce; every rank calls it in the same order)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -257,6 +259,9 @@ def main_b200(args, world, rank, local):
             eng.score_batch(wl.pairs)
         return eng.last_timing()
 
+    tuned = None
+    if not single:  # batches: schedule chosen by the autotuner on these shapes (outside the timing)
+        tuned, _ = eng.autotune(wl.pairs, trials=1)
     for _ in range(max(args.warmup, 0)):
         step()
     barrier(world)
@@ -307,7 +312,7 @@ def main_b200(args, world, rank, local):
                            "pairs": len(wl.pairs), "terms_per_step": terms_step,
                            "weights": [float(x) for x in wl.weights],
                            "l2": "inputs larger than L2 (each step streams its F tables from HBM)",
-                           "parallelism": f"independent pairs per rank x{world}"},
+                           "parallelism": f"independent pairs per rank x{world}", "autotuned": tuned},
                 "pct_maxplus_peak": 100.0 * value * 1e9 / peak,
                 "gpu_launches": launches, "wall_s": wall, "clocks": clocks, "roofline": roofline,
                 "cpu_baseline": cpu, "e2e": e2e, "batched": batched}
@@ -391,9 +396,11 @@ def measure_e2e(eng, wl, args, world):
 
 
 def measure_batched(eng):
-    """512 uneven pairs: one batched graph vs one fill per pair (both on this GPU)."""
+    """512 uneven pairs: one batched graph (schedule from the autotuner) vs one fill per pair (both
+    on this GPU)."""
     wl = W.batched_uneven(512, seed=4)
     eng.set_weights(wl.weights)
+    tuned, tune_ms = eng.autotune(wl.pairs, trials=1)
     eng.score_batch(wl.pairs)
     ms_b = []
     for _ in range(3):
@@ -408,7 +415,8 @@ def measure_batched(eng):
     return {"workload": wl.name, "pairs": len(wl.pairs), "pairs_per_s_batched": len(wl.pairs) / (mb * 1e-3),
             "pairs_per_s_per_pair_launch": len(wl.pairs) / (ms_e * 1e-3), "ms_batched": mb, "ms_per_pair_launch": ms_e,
             "speedup": ms_e / mb, "terms": wl.total_terms, "Gterms_per_s_batched": wl.total_terms / (mb * 1e-3) / 1e9,
-            "launches_per_pair_launch": launches_e, "wall_s_per_pair_pass": wall_e / 2}
+            "launches_per_pair_launch": launches_e, "wall_s_per_pair_pass": wall_e / 2,
+            "autotuned": tuned, "autotune_best_ms": tune_ms}
 
 
 def main():

@@ -65,6 +65,9 @@ def load_library():
     L.bpmax_gpu_profile_kernels.argtypes = [vp, vp, vp, vp]
     L.bpmax_gpu_maxplus_peak.argtypes = [vp, P(ctypes.c_double)]
     L.bpmax_gpu_score_noalloc.argtypes = [vp, c_long, vp, c_long, vp, vp, vp]
+    L.bpmax_gpu_set_tuning.argtypes = [vp, c_int, c_long]
+    L.bpmax_gpu_get_tuning.argtypes = [vp, c_int, P(c_long)]
+    L.bpmax_gpu_autotune.argtypes = [vp, c_int, vp, vp, vp, vp, c_int, vp, P(c_float)]
     for name in header_functions():
         if name not in ("bpmax_gpu_destroy", "bpmax_gpu_last_error", "bpmax_gpu_status_string"):
             getattr(L, name).restype = c_int
@@ -191,6 +194,26 @@ class Engine:
         grads = np.zeros((n, 12), dtype=np.float32)
         self._check(self._L.bpmax_gpu_grad_batch(self._ctx, n, p1, _ptr(Ms), p2, _ptr(Ns), _ptr(scores), _ptr(grads)))
         return scores, grads
+
+    TUNING_KEYS = {"r0_pairs_per_job": 0, "r0_merge_items": 1, "class_streams": 2}
+
+    def set_tuning(self, key: str, value: int) -> None:
+        self._check(self._L.bpmax_gpu_set_tuning(self._ctx, self.TUNING_KEYS[key], int(value)))
+
+    def get_tuning(self, key: str) -> int:
+        v = ctypes.c_long()
+        self._check(self._L.bpmax_gpu_get_tuning(self._ctx, self.TUNING_KEYS[key], ctypes.byref(v)))
+        return int(v.value)
+
+    def autotune(self, pairs, trials: int = 1):
+        """bpmax_gpu_autotune: times the candidate schedules on these pairs and keeps the fastest
+        for their shapes. Returns ({tunable: value}, fill ms)."""
+        n, p1, p2, Ms, Ns, keep = self._batch_args(pairs)
+        best = np.zeros(3, dtype=np.int64)
+        ms = ctypes.c_float()
+        self._check(self._L.bpmax_gpu_autotune(self._ctx, n, p1, _ptr(Ms), p2, _ptr(Ns), int(trials), _ptr(best),
+                                               ctypes.byref(ms)))
+        return {k: int(best[i]) for k, i in self.TUNING_KEYS.items()}, float(ms.value)
 
     def profile_kernels(self):
         """Per kernel kind (strand, r0, finalize): (ms, launches, terms) of an eager re-run of

@@ -11,12 +11,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -76,6 +78,7 @@ struct Plan {
     std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > 64 (first/count index this array)
     std::vector<CellJob> cell_jobs;
     std::vector<int> classes;  // distinct inner widths, ascending
+    int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
 };
@@ -93,8 +96,12 @@ struct bpmax_ctx {
     std::string err;
     DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
     int r0_occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class NB
+    // schedule tunables (bpmax_gpu_set_tuning / bpmax_gpu_autotune); a plan is built with the
+    // values current at build time, or with the values an autotune run stored for its shapes
     int r0_pairs_per_job = 1 << 20;                 // upper bound of k1 offset pairs per product job
     int r0_merge_items = 2;                         // cost of one job merge, in items, for job sizing
+    int class_streams = 1;                          // run the width classes of a batch on parallel streams
+    std::map<std::vector<int>, std::array<int, 3>> tuned;  // shape signature (Ms then Ns) -> tunables
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -147,11 +154,27 @@ int weights_ok(const float *w)
 long long align64(long long x) { return (x + 63) / 64 * 64; }
 
 // Builds the device layout and the per-diagonal job lists for the given pair shapes.
+std::vector<int> shape_key(const std::vector<int> &Ms, const std::vector<int> &Ns)
+{
+    std::vector<int> k(Ms);
+    k.insert(k.end(), Ns.begin(), Ns.end());
+    return k;
+}
+
 int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &Ns, Plan &P)
 {
     P = Plan();
     P.Ms = Ms;
     P.Ns = Ns;
+    P.pairs_per_job = ctx->r0_pairs_per_job;
+    P.merge_items = ctx->r0_merge_items;
+    P.class_streams = ctx->class_streams;
+    const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
+    if (tu != ctx->tuned.end()) {
+        P.pairs_per_job = tu->second[0];
+        P.merge_items = tu->second[1];
+        P.class_streams = tu->second[2];
+    }
     const int n = (int)Ms.size();
     long long f = 0, s = 0;
     int b = 0;
@@ -209,8 +232,8 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 const int NB = np / 8, G = R0_TAB_ITEMS[NB];
                 const long long P2 = (d + 1) / 2;  // offset pairs per cell
                 const long long resident = (long long)std::max(1, ctx->r0_occ[NB]) * ctx->sms;
-                const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(ctx->r0_pairs_per_job, qmin);
-                const long long q = r0_pairs_per_job(cells, P2, resident, qmin, qmax, ctx->r0_merge_items);
+                const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(P.pairs_per_job, qmin);
+                const long long q = r0_pairs_per_job(cells, P2, resident, qmin, qmax, P.merge_items);
                 Plan::Launch rl{d, np, (int)P.r0_jobs.size(), 0};
                 for (long long c0 = 0; c0 < P2; c0 += q)
                     for (int p = 0; p < n; ++p)
@@ -341,7 +364,7 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
     // pairs of different inner widths never interact: each width class runs its own chain of
     // diagonals on its own stream (parallel branches of the captured graph); profiling runs
     // serialise everything on the main stream so every launch can be timed
-    const bool fork = !(kp && kp->on) && P.classes.size() > 1;
+    const bool fork = !(kp && kp->on) && P.classes.size() > 1 && P.class_streams;
     auto stream_of = [&](int np) {
         if (!fork) return ctx->stream;
         const int k = (int)(std::find(P.classes.begin(), P.classes.end(), np) - P.classes.begin());
@@ -402,7 +425,13 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
             const std::vector<const int *> &s1s, const std::vector<const int *> &s2s)
 {
     int st;
-    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns)) {
+    const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
+    const std::array<int, 3> want = tu != ctx->tuned.end()
+                                        ? tu->second
+                                        : std::array<int, 3>{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams};
+    const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
+                             ctx->plan.class_streams == want[2];
+    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
         ctx->plan.graph = nullptr;
         ctx->plan_valid = false;
@@ -826,6 +855,87 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s)
     cudaFree(buf);
     if (e != cudaSuccess) return fail(ctx, BPMAX_ECUDA, "peak probe: %s", cudaGetErrorString(e));
     *terms_per_s = 3.0 * grid * block * (double)reps * 512.0 / (ms * 1e-3);
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    switch (key) {
+    case BPMAX_TUNE_R0_PAIRS_PER_JOB:
+        if (value < 1) return fail(ctx, BPMAX_EINVAL, "pairs per job must be >= 1");
+        ctx->r0_pairs_per_job = (int)std::min<long>(value, 1 << 20);
+        break;
+    case BPMAX_TUNE_R0_MERGE_ITEMS:
+        if (value < 0 || value > 1 << 20) return fail(ctx, BPMAX_EINVAL, "merge cost out of range");
+        ctx->r0_merge_items = (int)value;
+        break;
+    case BPMAX_TUNE_CLASS_STREAMS:
+        ctx->class_streams = value != 0;
+        break;
+    default: return fail(ctx, BPMAX_EINVAL, "unknown tuning key %d", key);
+    }
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value)
+{
+    if (!ctx || !value) return BPMAX_EINVAL;
+    switch (key) {
+    case BPMAX_TUNE_R0_PAIRS_PER_JOB: *value = ctx->r0_pairs_per_job; break;
+    case BPMAX_TUNE_R0_MERGE_ITEMS: *value = ctx->r0_merge_items; break;
+    case BPMAX_TUNE_CLASS_STREAMS: *value = ctx->class_streams; break;
+    default: return BPMAX_EINVAL;
+    }
+    return BPMAX_OK;
+}
+
+int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms, const int *const *seq2s,
+                       const long *Ns, int trials, long *best, float *best_ms)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (num_pairs < 1 || !Ms || !Ns) return fail(ctx, BPMAX_EINVAL, "empty batch");
+    std::vector<int> vm(num_pairs), vn(num_pairs);
+    for (int p = 0; p < num_pairs; ++p) {
+        vm[p] = (int)Ms[p];
+        vn[p] = (int)Ns[p];
+    }
+    const std::vector<int> key = shape_key(vm, vn);
+    ctx->tuned.erase(key);
+    const int saved[3] = {ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams};
+    std::set<int> classes;
+    for (int n : vn) classes.insert(padded_width(n));
+    const int jobs_cand[] = {8, 32, 1 << 20}, merge_cand[] = {1, 4}, streams_cand[] = {1, 0};
+    float best_t = -1.f;
+    std::array<int, 3> best_cfg{saved[0], saved[1], saved[2]};
+    int st = BPMAX_OK;
+    for (int sc : streams_cand) {
+        if (sc == 0 && classes.size() < 2) continue;  // one class: the stream setting changes nothing
+        for (int jc : jobs_cand)
+            for (int mc : merge_cand) {
+                ctx->r0_pairs_per_job = jc;
+                ctx->r0_merge_items = mc;
+                ctx->class_streams = sc;
+                float t = -1.f;
+                for (int r = 0; r < 1 + std::max(1, trials) && st == BPMAX_OK; ++r) {  // first run captures the graph
+                    st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
+                    if (st == BPMAX_OK && r > 0 && (t < 0 || ctx->last_ms < t)) t = ctx->last_ms;
+                }
+                if (st != BPMAX_OK) break;
+                if (best_t < 0 || t < best_t) {
+                    best_t = t;
+                    best_cfg = {jc, mc, sc};
+                }
+            }
+    }
+    ctx->r0_pairs_per_job = saved[0];
+    ctx->r0_merge_items = saved[1];
+    ctx->class_streams = saved[2];
+    if (st != BPMAX_OK) return st;
+    ctx->tuned[key] = best_cfg;
+    if (best)
+        for (int k = 0; k < 3; ++k) best[k] = best_cfg[k];
+    if (best_ms) *best_ms = best_t;
     return BPMAX_OK;
 }
 

@@ -88,6 +88,28 @@ int bpmax_gpu_score_each(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s,
 int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
                          const int *const *seq2s, const long *Ns, float *scores, float *grads);
 
+/* Schedule tunables of later fills (no reference counterpart: the reference's tuning knobs are its
+ * compile-time tile sizes and the MR/NR/P arguments of bpmax(), V3/bpmax.c:129).
+ *   BPMAX_TUNE_R0_PAIRS_PER_JOB  upper bound of k1 offset pairs (w, d-1-w) per product job (>= 1)
+ *   BPMAX_TUNE_R0_MERGE_ITEMS    cost of one job's merge, in items, used to size the jobs of a diagonal
+ *   BPMAX_TUNE_CLASS_STREAMS     1: width classes of a batch run as parallel graph branches; 0: one chain */
+enum bpmax_tuning_key {
+    BPMAX_TUNE_R0_PAIRS_PER_JOB = 0,
+    BPMAX_TUNE_R0_MERGE_ITEMS = 1,
+    BPMAX_TUNE_CLASS_STREAMS = 2
+};
+int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value);
+int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value);
+
+/* Autotuner: fills the given pairs under each candidate setting of the three tunables (pairs per
+ * job 8 / 32 / unbounded, merge cost 1 / 4, class streams on / off when the batch has several
+ * width classes), timing `trials` graph replays of each after one capture run, and keeps the
+ * fastest setting for these shapes: later fills of the same shapes use it. best (may be NULL)
+ * receives the 3 chosen values in key order, best_ms (may be NULL) the fill time in ms. Results of
+ * every fill are unchanged by any setting (bit for bit). No reference counterpart. */
+int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
+                       const int *const *seq2s, const long *Ns, int trials, long *best, float *best_ms);
+
 /* Device time in milliseconds of the last fill call's kernels (CUDA events on the context's
  * stream), and the number of kernel launches it issued. */
 int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches);

@@ -162,3 +162,46 @@ def test_batched_mixed_widths(eng, oracle_mod):
     exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
                    dtype=np.float32)
     assert np.array_equal(bits(got), bits(exp))
+
+
+def test_tuning_settings_keep_results(eng, oracle_mod):
+    """Every schedule setting changes how the work is cut, never a result bit."""
+    pairs = [W.pair(m, n, 80 + i) for i, (m, n) in enumerate([(23, 61), (17, 30), (9, 12), (31, 64), (6, 45)])]
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
+                   dtype=np.float32)
+    saved = {k: eng.get_tuning(k) for k in ("r0_pairs_per_job", "r0_merge_items", "class_streams")}
+    try:
+        for ppj, merge, streams in [(1, 0, 1), (3, 16, 0), (1 << 20, 2, 1), (2, 1, 0)]:
+            eng.set_tuning("r0_pairs_per_job", ppj)
+            eng.set_tuning("r0_merge_items", merge)
+            eng.set_tuning("class_streams", streams)
+            assert np.array_equal(bits(eng.score_batch(pairs)), bits(exp))
+            F, _ = eng.fill_compact(*pairs[0])
+            Fo, _, _ = oracle_mod.fill(*pairs[0], W.INTEGER_WEIGHTS)
+            assert np.array_equal(bits(F), bits(Fo))
+    finally:
+        for k, v in saved.items():
+            eng.set_tuning(k, v)
+
+
+def test_autotune_picks_a_setting_and_keeps_results(eng, oracle_mod):
+    wl = W.batched_uneven(num_pairs=10, seed=79, m_range=(2, 28), n_range=(1, 64))
+    eng.set_weights(wl.weights)
+    before = eng.score_batch(wl.pairs)
+    best, ms = eng.autotune(wl.pairs, trials=1)
+    assert best["r0_pairs_per_job"] in (8, 32, 1 << 20) and best["r0_merge_items"] in (1, 4)
+    assert best["class_streams"] in (0, 1) and ms > 0
+    after = eng.score_batch(wl.pairs)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, wl.weights)[0], len(a), len(b)) for a, b in wl.pairs],
+                   dtype=np.float32)
+    assert np.array_equal(bits(before), bits(exp)) and np.array_equal(bits(after), bits(exp))
+
+
+def test_tuning_rejects_bad_values(eng):
+    from bpmax_b200 import BpmaxError
+
+    with pytest.raises(BpmaxError):
+        eng.set_tuning("r0_pairs_per_job", 0)
+    with pytest.raises(BpmaxError):
+        eng._check(eng._L.bpmax_gpu_set_tuning(eng._ctx, 7, 1))
