@@ -69,7 +69,9 @@ struct R0Cfg {
     static constexpr int STAGE_BYTES = STAGE * 16;
     static constexpr int NBLK = NB * (NB + 1) / 2;
     static constexpr int RED_WORDS = 65 * NBLK;             // job-merge tile, one 8x8 block per 65 words
-    static constexpr int STAGE_BUDGET = 75 * 1024 - 4 * RED_WORDS - 4 * NBLK - 64;  // 3 CTAs per SM
+    // shared-memory budget of the stages: 3 CTAs per SM; 4 for the 96-thread NB = 7 CTAs (their
+    // registers allow it, and 12 resident warps beat a fourth stage)
+    static constexpr int STAGE_BUDGET = (NB == 7 ? 55 : 75) * 1024 - 4 * RED_WORDS - 4 * NBLK - 64;
     static constexpr int STAGES = STAGE_BYTES * 4 <= STAGE_BUDGET ? 4 : (STAGE_BYTES * 3 <= STAGE_BUDGET ? 3 : 2);
     static constexpr int ITEM_TX = 2 * IMG * 16;            // bytes landing per item
     static constexpr int MINB = THREADS <= 64 ? 6 : (THREADS <= 96 ? 4 : 3);
