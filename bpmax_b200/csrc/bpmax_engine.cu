@@ -79,6 +79,7 @@ struct Plan {
     std::vector<CellJob> cell_jobs;
     std::vector<int> classes;  // distinct inner widths, ascending
     int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
+    std::vector<cudaEvent_t> diag_ev;  // one pair only: outer diagonal d finalized (recorded by the graph)
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
 };
@@ -90,6 +91,7 @@ struct bpmax_ctx {
     int sms = 148;
     cudaStream_t stream = nullptr;
     cudaStream_t class_stream[8] = {};  // MAX_CLASS_STREAMS
+    cudaStream_t aux_stream = nullptr;  // reference-layout conversion and copy-out, overlapped with the fill
     cudaEvent_t fork_ev = nullptr, join_ev[8] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
@@ -409,6 +411,9 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
             default: launch_fin<8>(ctx, L, st); break;
             }
         }
+        // outer diagonal d is final: rows of the reference layout that end on it can be copied out
+        if (!P.diag_ev.empty() && !(kp && kp->on))
+            CK(cudaEventRecordWithFlags(P.diag_ev[d], ctx->stream, cudaEventRecordExternal));
     }
     for (int k = 0; k < nstreams; ++k) {  // join the class chains back into the main stream
         CK(cudaEventRecord(ctx->join_ev[k], ctx->class_stream[k]));
@@ -434,9 +439,15 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
     if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
         ctx->plan.graph = nullptr;
+        for (cudaEvent_t e : ctx->plan.diag_ev) cudaEventDestroy(e);
+        ctx->plan.diag_ev.clear();
         ctx->plan_valid = false;
         if ((st = build_plan(ctx, Ms, Ns, ctx->plan)) != BPMAX_OK) return st;
         Plan &P = ctx->plan;
+        if (P.pairs.size() == 1) {
+            P.diag_ev.assign(P.maxM, nullptr);
+            for (auto &e : P.diag_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
         if ((st = ensure(ctx, ctx->F, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
         if (P.any_wide && (st = ensure(ctx, ctx->FT, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->errflag, sizeof(int))) != BPMAX_OK) return st;
@@ -470,8 +481,8 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
     return BPMAX_OK;
 }
 
-// Runs the fill of the current plan (graph captured on first use) and times it.
-int run_fill(bpmax_ctx *ctx)
+// Launches the fill of the current plan (graph captured on first use) on the context's stream.
+int launch_fill(bpmax_ctx *ctx)
 {
     Plan &P = ctx->plan;
     int st;
@@ -496,6 +507,13 @@ int run_fill(bpmax_ctx *ctx)
     gather_scores_kernel<<<((int)P.pairs.size() + 127) / 128, 128, 0, ctx->stream>>>(
         (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)P.pairs.size(), (float *)ctx->scores.p);
     CK(cudaGetLastError());
+    return BPMAX_OK;
+}
+
+// Waits for the fill launched by launch_fill, reads its error word and times it.
+int finish_fill(bpmax_ctx *ctx)
+{
+    Plan &P = ctx->plan;
     int errv = 0;
     CK(cudaMemcpyAsync(&errv, ctx->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev1));
@@ -504,6 +522,12 @@ int run_fill(bpmax_ctx *ctx)
     ctx->last_launches = P.launches + 1;  // + the score gather
     if (errv) return fail(ctx, BPMAX_ETIMEOUT, "a product kernel gave up waiting for its operand copies");
     return BPMAX_OK;
+}
+
+int run_fill(bpmax_ctx *ctx)
+{
+    const int st = launch_fill(ctx);
+    return st ? st : finish_fill(ctx);
 }
 
 int check_pair(bpmax_ctx *ctx, const int *s1, long M, const int *s2, long N)
@@ -519,7 +543,7 @@ int check_pair(bpmax_ctx *ctx, const int *s1, long M, const int *s2, long N)
 }
 
 int fill_pairs(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms, const int *const *seq2s,
-               const long *Ns)
+               const long *Ns, bool async = false)
 {
     if (!ctx) return BPMAX_EINVAL;
     if (num_pairs < 1 || !seq1s || !seq2s || !Ms || !Ns) return fail(ctx, BPMAX_EINVAL, "empty batch");
@@ -536,7 +560,7 @@ int fill_pairs(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const lon
     CK(cudaSetDevice(ctx->device));
     int st = prepare(ctx, vm, vn, a, b);
     if (st) return st;
-    return run_fill(ctx);
+    return async ? launch_fill(ctx) : run_fill(ctx);
 }
 
 int ensure_host_stage(bpmax_ctx *ctx, size_t bytes)
@@ -605,6 +629,7 @@ int bpmax_gpu_create(int device, bpmax_ctx **out)
         cudaEventCreateWithFlags(&ctx->stage_ev[1], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess)
         st = BPMAX_ECUDA;
+    if (st == BPMAX_OK && cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking) != cudaSuccess) st = BPMAX_ECUDA;
     for (int k = 0; k < MAX_CLASS_STREAMS && st == BPMAX_OK; ++k)
         if (cudaStreamCreateWithFlags(&ctx->class_stream[k], cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
@@ -642,6 +667,8 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    for (cudaEvent_t e : ctx->plan.diag_ev) cudaEventDestroy(e);
+    if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
     for (int k = 0; k < MAX_CLASS_STREAMS; ++k) {
         if (ctx->class_stream[k]) cudaStreamDestroy(ctx->class_stream[k]);
         if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
@@ -729,19 +756,26 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
     if (M < 1 || N < 8 || N_tile < 4) return fail(ctx, BPMAX_EINVAL, "The value of parameters are not valid.");
     const long Ns = (N + N_tile - 1) / N_tile;
     if (Ns < 2) return fail(ctx, BPMAX_EINVAL, "The value of parameters are not valid. (N_sec=%ld < 2)", Ns);
-    int st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N);
-    if (st) return st;
-    if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
-    if (!F_lin) return BPMAX_OK;
+    if (!F_lin) {
+        int st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N);
+        if (st) return st;
+        if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+        return BPMAX_OK;
+    }
     const long long cell_f = (long long)Ns * Ns * (N_tile + 1) * N_tile;
-    // outer row i1 of the reference layout: cells (i1, i1..M-1) are contiguous
+    // outer row i1 of the reference layout: cells (i1, i1..M-1) are contiguous; it is final once
+    // outer diagonal M-1-i1 is, so rows are converted and copied out from the last one up while
+    // the fill still runs (aux stream, waiting on the per-diagonal events the graph records)
     const long long row_max = (long long)M * cell_f;
+    int st;
     if ((st = ensure(ctx, ctx->conv, 2 * row_max * sizeof(float))) != BPMAX_OK) return st;
     const bool pinned = is_pinned(F_lin);
     if (!pinned && (st = ensure_host_stage(ctx, row_max * sizeof(float))) != BPMAX_OK) return st;
+    if ((st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N, true)) != BPMAX_OK) return st;
+    const std::vector<cudaEvent_t> &dev = ctx->plan.diag_ev;
     std::vector<long long> pending_n(2, 0);
     std::vector<float *> pending_dst(2, nullptr);
-    for (long i1 = 0; i1 < M; ++i1) {
+    for (long i1 = M - 1; i1 >= 0; --i1) {
         const int slot = (int)(i1 & 1);
         float *dbuf = (float *)ctx->conv.p + slot * row_max;
         const long long n_out = (M - i1) * cell_f;
@@ -751,14 +785,16 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
             memcpy(pending_dst[slot], ctx->host_stage[slot], pending_n[slot] * sizeof(float));
             pending_dst[slot] = nullptr;
         }
-        to_reference_row_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>(
+        CK(cudaStreamWaitEvent(ctx->aux_stream, dev[M - 1 - i1], 0));
+        to_reference_row_kernel<<<4 * ctx->sms, 256, 0, ctx->aux_stream>>>(
             (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)N_tile, (int)Ns, (int)i1, n_out, dbuf);
         CK(cudaGetLastError());
         if (pinned) {
-            CK(cudaMemcpyAsync(dst, dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(dst, dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->aux_stream));
         } else {
-            CK(cudaMemcpyAsync(ctx->host_stage[slot], dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaEventRecord(ctx->stage_ev[slot], ctx->stream));
+            CK(cudaMemcpyAsync(ctx->host_stage[slot], dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost,
+                               ctx->aux_stream));
+            CK(cudaEventRecord(ctx->stage_ev[slot], ctx->aux_stream));
             pending_dst[slot] = dst;
             pending_n[slot] = n_out;
         }
@@ -768,7 +804,9 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
             CK(cudaEventSynchronize(ctx->stage_ev[slot]));
             memcpy(pending_dst[slot], ctx->host_stage[slot], pending_n[slot] * sizeof(float));
         }
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaStreamSynchronize(ctx->aux_stream));
+    if ((st = finish_fill(ctx)) != BPMAX_OK) return st;
+    if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
     return BPMAX_OK;
 }
 
