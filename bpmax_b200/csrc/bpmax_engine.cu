@@ -878,7 +878,7 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s)
     if (!ctx || !terms_per_s) return BPMAX_EINVAL;
     CK(cudaSetDevice(ctx->device));
     float *buf = nullptr;
-    const int grid = ctx->sms * 8, block = 128, reps = 1000;
+    const int grid = ctx->sms * 8, block = 128, reps = 250;
     CK(cudaMalloc(&buf, (size_t)grid * block * sizeof(float) + 64 * sizeof(float)));
     std::vector<float> h(64);
     for (int i = 0; i < 64; ++i) h[i] = (float)(i % 17);
@@ -892,7 +892,7 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s)
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     cudaFree(buf);
     if (e != cudaSuccess) return fail(ctx, BPMAX_ECUDA, "peak probe: %s", cudaGetErrorString(e));
-    *terms_per_s = 3.0 * grid * block * (double)reps * 512.0 / (ms * 1e-3);
+    *terms_per_s = 3.0 * grid * block * (double)reps * (8.0 * MAXPLUS_PEAK_CHAINS) / (ms * 1e-3);
     return BPMAX_OK;
 }
 

@@ -367,49 +367,39 @@ __global__ void gather_scores_kernel(const PairDesc *__restrict__ pairs, const f
 }
 
 // ------------------------------------------------------------------------------------------
-// Max-plus issue ceiling: an 8x8 register tile takes 4 candidates per 2 three-input max steps
-// from four different operand pairings before the operands are perturbed, so nothing is
-// loop-invariant and the perturbation costs ~3% of the instructions. Each iteration is 512
-// candidates per thread.
+// Max-plus issue ceiling: the product kernel's instruction mix with nothing to share between
+// candidates. Each step of a chain is one packed add (two candidate sums, the running operand
+// plus a step) and one 3-input max that merges both sums into the chain's maximum; every sum is
+// new (the running operand changes each step) and is consumed once, so the compiler can neither
+// hoist nor reuse an add. MAXPLUS_PEAK_CHAINS independent chains per thread give the schedulers
+// the same independent work as the product kernel's 8x8 tile. Each iteration is
+// 4 * 2 * MAXPLUS_PEAK_CHAINS candidates per thread.
 // ------------------------------------------------------------------------------------------
+constexpr int MAXPLUS_PEAK_CHAINS = 16;
 __global__ void __launch_bounds__(128) maxplus_peak_kernel(const float *__restrict__ in, float *__restrict__ out,
                                                            int reps)
 {
-    float a[8], b[8], c[8], e[8], acc[8][8];
+    constexpr int CH = MAXPLUS_PEAK_CHAINS;
+    float2 p[CH], q[CH];
+    float m[CH];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        a[i] = in[(threadIdx.x + i) & 63];
-        b[i] = in[(threadIdx.x + 8 + i) & 63];
-        c[i] = in[(threadIdx.x + 16 + i) & 63];
-        e[i] = in[(threadIdx.x + 24 + i) & 63];
+    for (int i = 0; i < CH; ++i) {
+        p[i] = make_float2(in[(threadIdx.x + i) & 63], in[(threadIdx.x + 2 * i + 1) & 63]);
+        q[i] = make_float2(in[(threadIdx.x + 3 * i + 2) & 63] * 1e-7f, in[(threadIdx.x + 5 * i + 3) & 63] * 1e-7f);
+        m[i] = NEG_INF;
     }
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = NEG_INF;
     for (int r = 0; r < reps; ++r) {
 #pragma unroll
         for (int s = 0; s < 4; ++s)
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int jj = (j + s) & 7;
-                    acc[i][j] = fmax3(acc[i][j], a[i] + b[jj], c[i] + e[jj]);
-                }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            a[i] *= 0.999f;
-            b[i] *= 1.001f;
-            c[i] *= 0.998f;
-            e[i] *= 1.002f;
-        }
+            for (int i = 0; i < CH; ++i) {
+                p[i] = __fadd2_rn(p[i], q[i]);
+                m[i] = fmax3(m[i], p[i].x, p[i].y);
+            }
     }
     float s = 0.f;
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) s += acc[i][j];
+    for (int i = 0; i < CH; ++i) s += p[i].x + p[i].y + m[i];
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 

@@ -28,9 +28,16 @@
 // offsets in pairs (w, d-1-w), the offset pair p = min(w, d-1-w) being the same for both uses,
 // and the job list is ordered by offset pair.
 //
-// The inner loop adds in pairs: (a, a) + (b[j], b[j+1]) with one packed fp32 add (__fadd2_rn,
-// round-to-nearest like the scalar add), and merges four candidates per accumulator with two
-// 3-input max steps. At the end of a job the partial maxima of all tasks first meet in a shared
+// The inner loop takes 4 k per step: the 4 rows of the shifted B block in registers, then one A
+// row at a time (its 4 operands live only for that row's 32 candidates, which keeps the kernel
+// inside 168 registers without spills). It adds in pairs: (a, a) + (b[j], b[j+1]) with one packed
+// fp32 add (__fadd2_rn, round-to-nearest like the scalar add), and merges four candidates per
+// accumulator with two 3-input max steps.
+// Warp programs (width 64): the lane table groups the tasks by kind, one kind per warp. Tasks
+// with kb == bi < bj (A block on the diagonal) skip the k pairs a row meets only below the
+// subdiagonal, tasks with bi < kb == bj (shifted B block on the diagonal) skip the column pairs a k
+// pair meets only below the diagonal; the skipped candidates are all -inf, so every maximum is
+// unchanged, and those warps issue 92 and 80 of the 128 steps of a full task. At the end of a job the partial maxima of all tasks first meet in a shared
 // tile of the cell's blocks (shared atomicMax; blocks at a pitch of 65 words so the lanes of a
 // warp hit distinct banks), then the tile merges into F(i1, j1) with coalesced global atomicMax,
 // consecutive lanes on consecutive words (max on the int bit patterns is exact: all values are
@@ -82,6 +89,11 @@ struct R0Cfg {
     static constexpr int OFF_CNT = OFF_BAR + 8 * STAGES;  // per stage: warps done with it
     static constexpr size_t SMEM = (size_t)OFF_CNT + 4 * STAGES;
     static constexpr int WARPS = THREADS / 32;
+    // warp program of each warp slot, 2 bits per slot (0 full task, 1 diagonal A, 2 diagonal B)
+    static constexpr bool HAS_ROLES = R0_TAB_HAS_ROLES[NB];
+    static constexpr unsigned ROLE_BITS = R0_TAB_ROLE[NB][0] | R0_TAB_ROLE[NB][1] << 2 | R0_TAB_ROLE[NB][2] << 4 |
+                                          R0_TAB_ROLE[NB][3] << 6 | R0_TAB_ROLE[NB][4] << 8 | R0_TAB_ROLE[NB][5] << 10 |
+                                          R0_TAB_ROLE[NB][6] << 12 | R0_TAB_ROLE[NB][7] << 14;
     static_assert(STAGE_BYTES % 16 == 0 && OFF_RED % 16 == 0 && OFF_BAR % 8 == 0, "shared-memory alignment");
     static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
 };
@@ -118,6 +130,60 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
                  : "memory");
 }
 
+// One lane's task over one item: acc[i][j] = max over the task's k of A[i][k] + Bs[k][j].
+// ROLE 0 (full) evaluates all 8 k; ROLE 1 (A block on the diagonal, kb == bi) evaluates the k
+// pair p = (2p, 2p+1) only for rows i <= 2p+2, since A[i][k] = -inf for k < i-1; ROLE 2 (shifted B
+// block on the diagonal, kb == bj) evaluates k pair p only for column pairs jp >= p, since
+// Bs[k][j] = -inf for k > j. The skipped candidates are all -inf, so the maxima are unchanged.
+template <int ROLE>
+__device__ __forceinline__ bool r0_pair_used(int i, int jp, int p)
+{
+    return ROLE == 1 ? i <= 2 * p + 2 : (ROLE == 2 ? jp >= p : true);
+}
+template <int ROLE>
+__device__ __forceinline__ void r0_task(const float *__restrict__ As, const float *__restrict__ Bs, float (&acc)[8][8])
+{
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        float2 bv[4][4];  // bv[k][jp] = (Bs[4q+k][2jp], Bs[4q+k][2jp+1])
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int row = 4 * q + k, ro = 8 * row + (row == 7 ? 4 : 0);  // row 7: next block / S1 piece
+            if (r0_pair_used<ROLE>(0, 0, 2 * q + k / 2) || r0_pair_used<ROLE>(0, 1, 2 * q + k / 2)) {  // row 0 widest
+                const float4 t0 = *reinterpret_cast<const float4 *>(Bs + ro);
+                bv[k][0] = make_float2(t0.x, t0.y); bv[k][1] = make_float2(t0.z, t0.w);
+            }
+            const float4 t1 = *reinterpret_cast<const float4 *>(Bs + ro + 4);
+            bv[k][2] = make_float2(t1.x, t1.y); bv[k][3] = make_float2(t1.z, t1.w);
+        }
+        // one A row at a time: the row's 4 operands are live only for its 32 candidates
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (!r0_pair_used<ROLE>(i, 3, 2 * q) && !r0_pair_used<ROLE>(i, 3, 2 * q + 1)) continue;
+            const float4 t = *reinterpret_cast<const float4 *>(As + 8 * i + 4 * q);
+            const float av[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+            for (int jp = 0; jp < 4; ++jp) {
+                const bool u0 = r0_pair_used<ROLE>(i, jp, 2 * q), u1 = r0_pair_used<ROLE>(i, jp, 2 * q + 1);
+                if (u0 && u1) {
+                    const float2 s0 = __fadd2_rn(make_float2(av[0], av[0]), bv[0][jp]);
+                    const float2 s1 = __fadd2_rn(make_float2(av[1], av[1]), bv[1][jp]);
+                    const float2 s2 = __fadd2_rn(make_float2(av[2], av[2]), bv[2][jp]);
+                    const float2 s3 = __fadd2_rn(make_float2(av[3], av[3]), bv[3][jp]);
+                    acc[i][2 * jp] = fmax3(fmax3(acc[i][2 * jp], s0.x, s1.x), s2.x, s3.x);
+                    acc[i][2 * jp + 1] = fmax3(fmax3(acc[i][2 * jp + 1], s0.y, s1.y), s2.y, s3.y);
+                } else if (u0 || u1) {
+                    const int k0 = u0 ? 0 : 2;
+                    const float2 s0 = __fadd2_rn(make_float2(av[k0], av[k0]), bv[k0][jp]);
+                    const float2 s1 = __fadd2_rn(make_float2(av[k0 + 1], av[k0 + 1]), bv[k0 + 1][jp]);
+                    acc[i][2 * jp] = fmax3(acc[i][2 * jp], s0.x, s1.x);
+                    acc[i][2 * jp + 1] = fmax3(acc[i][2 * jp + 1], s0.y, s1.y);
+                }
+            }
+        }
+    }
+}
+
 template <int NB>
 __global__ void __launch_bounds__(R0Cfg<NB>::THREADS, R0Cfg<NB>::MINB)
 r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs, float *__restrict__ F, int d,
@@ -152,7 +218,8 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         red_dst[tid] = 4 * (c_img_colbase[NB][bj_] + 17 * bi_);
     }
 
-    // this thread's task and its float offsets inside an item
+    // the warp's program (uniform over its lanes) and this thread's task
+    const int role = C::HAS_ROLES ? (int)(C::ROLE_BITS >> (2 * (tid >> 5))) & 3 : 0;
     const unsigned char *lt = c_r0_lane[NB - 1][tid];
     const bool has_task = lt[0] != 255;
     const int tg = has_task ? lt[0] : 0, bi = lt[1], bj = lt[2], kb = lt[3];
@@ -168,15 +235,17 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
 
     const unsigned smem_base = smem_u32(smem);
     const int lane = tid & 31;
-    // announces the bytes of iteration `it` of job `jb` on stage s's mbarrier (one thread, before
-    // any copy of that iteration is issued)
-    auto expect = [&](int s, const R0Job &jb, int it) {
-        const int valid = min(C::G, r0_job_items(jb, d) - it * C::G);
+    // announces the bytes of iteration `it` of a job of `items` items on stage s's mbarrier (one
+    // thread, before any copy of that iteration is issued)
+    auto expect = [&](int s, int items, int it) {
+        const int valid = min(C::G, items - it * C::G);
         mbar_arrive_tx(smem_u32(bars + s), (unsigned)(valid * C::ITEM_TX));
     };
-    // issues the copies (whole cell images) of iteration `it` of job `jb` into stage s, spread
-    // over the threads first..first+count-1
-    auto issue = [&](int s, const R0Job &jb, int it, int me, int count) {
+    // issues the copies (whole cell images) of iteration `it` of job j into stage s, spread over
+    // the threads me, me+count, ... (the job record is re-read here: positions are kept as indices,
+    // not records, to leave the registers to the product tile)
+    auto issue = [&](int s, int j, int it, int me, int count) {
+        const R0Job jb = jobs[j];
         const PairDesc pd = pairs[jb.pair];
         const int M = pd.M, j1 = jb.i1 + d;
         const int valid = min(C::G, r0_job_items(jb, d) - it * C::G);
@@ -190,33 +259,31 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         }
     };
 
-    // consumer position (jid, job, it) and producer position (pj, pjob, pit), S iterations ahead;
-    // every warp advances both the same way, so all agree on which iteration each stage holds
-    R0Job job = jobs[jid];
-    int n_it = (r0_job_items(job, d) + C::G - 1) / C::G, it = 0;
-    int pj = jid, pit = 0;
-    R0Job pjob = job;
-    auto advance = [&](int &j_, R0Job &jb_, int &it_) {
-        if (++it_ * C::G >= r0_job_items(jb_, d)) {
+    // consumer position (job jid of `items` items, iteration it) and producer position (pj, pitems,
+    // pit), S iterations ahead; every warp advances both the same way, so all agree on which
+    // iteration each stage holds
+    int items = r0_job_items(jobs[jid], d), it = 0;
+    int pj = jid, pit = 0, pitems = items;
+    auto advance = [&](int &j_, int &items_, int &it_) {
+        if (++it_ * C::G >= items_) {
             it_ = 0;
             j_ += gridDim.x;
-            if (j_ < njobs) jb_ = jobs[j_];
+            if (j_ < njobs) items_ = r0_job_items(jobs[j_], d);
         }
     };
     if (tid == 0) {  // expected bytes of the first S iterations (every stage starts free)
-        int j_ = pj, it_ = pit;
-        R0Job jb_ = pjob;
+        int j_ = pj, it_ = pit, items_ = pitems;
         for (int s = 0; s < S && j_ < njobs; ++s) {
-            expect(s, jb_, it_);
-            advance(j_, jb_, it_);
+            expect(s, items_, it_);
+            advance(j_, items_, it_);
         }
     }
     __syncthreads();
 #pragma unroll 1
     for (int s = 0; s < S; ++s)
         if (pj < njobs) {
-            issue(s, pjob, pit, tid, C::THREADS);
-            advance(pj, pjob, pit);
+            issue(s, pj, pit, tid, C::THREADS);
+            advance(pj, pitems, pit);
         }
 
     float acc[8][8];
@@ -230,7 +297,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
     bool bad = false;    // an mbarrier wait ran out: skip waits and work, leave at the next job end
 #pragma unroll 1
     while (true) {
-        const bool active = has_task && it * C::G + tg < r0_job_items(job, d);
+        const bool active = has_task && it * C::G + tg < items;
         if (!bad && !mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u)) {
             atomicExch(err, 1);
             bad = true;
@@ -239,35 +306,12 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         if (active && !bad) {
             const float *item = smem + (size_t)stage * C::STAGE * 4 + tg * C::ITEM * 4;
             const float *As = item + a_off, *Bs = item + b_off;
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                float av[8][4];
-                float2 bv[4][4];  // bv[k][jp] = (Bs[4q+k][2jp], Bs[4q+k][2jp+1])
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    const float4 t = *reinterpret_cast<const float4 *>(As + 8 * i + 4 * q);
-                    av[i][0] = t.x; av[i][1] = t.y; av[i][2] = t.z; av[i][3] = t.w;
-                }
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int row = 4 * q + k, ro = 8 * row + (row == 7 ? 4 : 0);  // row 7: next block / S1 piece
-                    const float4 t0 = *reinterpret_cast<const float4 *>(Bs + ro);
-                    const float4 t1 = *reinterpret_cast<const float4 *>(Bs + ro + 4);
-                    bv[k][0] = make_float2(t0.x, t0.y); bv[k][1] = make_float2(t0.z, t0.w);
-                    bv[k][2] = make_float2(t1.x, t1.y); bv[k][3] = make_float2(t1.z, t1.w);
-                }
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-#pragma unroll
-                    for (int jp = 0; jp < 4; ++jp) {
-                        const float2 s0 = __fadd2_rn(make_float2(av[i][0], av[i][0]), bv[0][jp]);
-                        const float2 s1 = __fadd2_rn(make_float2(av[i][1], av[i][1]), bv[1][jp]);
-                        const float2 s2 = __fadd2_rn(make_float2(av[i][2], av[i][2]), bv[2][jp]);
-                        const float2 s3 = __fadd2_rn(make_float2(av[i][3], av[i][3]), bv[3][jp]);
-                        acc[i][2 * jp] = fmax3(fmax3(acc[i][2 * jp], s0.x, s1.x), s2.x, s3.x);
-                        acc[i][2 * jp + 1] = fmax3(fmax3(acc[i][2 * jp + 1], s0.y, s1.y), s2.y, s3.y);
-                    }
-            }
+            if (!C::HAS_ROLES || role == 0)
+                r0_task<0>(As, Bs, acc);
+            else if (role == 1)
+                r0_task<1>(As, Bs, acc);
+            else
+                r0_task<2>(As, Bs, acc);
             if (kb == bi) {  // k = 8bi-1 term of row 8bi: S1(i1,k1) + B[8bi][j2]
                 const float s1a = item[s1_off];
                 const float4 r0 = *reinterpret_cast<const float4 *>(item + r3_off);
@@ -285,15 +329,16 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         if (last && pj < njobs) {
             if (lane == 0) {
                 done_cnt[stage] = 0;
-                expect(stage, pjob, pit);
+                expect(stage, pitems, pit);
             }
             __syncwarp();
-            issue(stage, pjob, pit, lane, 32);
+            issue(stage, pj, pit, lane, 32);
         } else if (last && lane == 0) {
             done_cnt[stage] = 0;
         }
-        if (pj < njobs) advance(pj, pjob, pit);
-        if (++it >= n_it) {  // job done: merge the partial maxima of all tasks into F(i1, i1+d)
+        if (pj < njobs) advance(pj, pitems, pit);
+        if (++it * C::G >= items) {  // job done: merge the partial maxima of all tasks into F(i1, i1+d)
+            const R0Job job = jobs[jid];
             const PairDesc pd = pairs[job.pair];
             if (has_task) {
 #pragma unroll
@@ -319,8 +364,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
             __syncthreads();  // the tile is clear before any warp merges its next job into it
             jid += gridDim.x;
             if (jid >= njobs) break;
-            job = jobs[jid];
-            n_it = (r0_job_items(job, d) + C::G - 1) / C::G;
+            items = r0_job_items(jobs[jid], d);
             it = 0;
         }
         stage = (stage + 1) % S;

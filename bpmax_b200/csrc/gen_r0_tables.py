@@ -27,9 +27,45 @@ import random
 # (threads per CTA, items per iteration) for each NB: G*TASKS(NB) lanes work, the rest idle
 CFG = {1: (64, 64), 2: (96, 24), 3: (128, 12), 4: (128, 6), 5: (128, 3), 6: (128, 2), 7: (96, 1), 8: (128, 1)}
 
+# Warp programs. FULL: the whole 8x8x8 task. DIAG_A: tasks with kb == bi (A block on the diagonal),
+# k pair (2p, 2p+1) only for rows i <= 2p+2 (the other rows meet -inf below the subdiagonal).
+# DIAG_B: tasks with kb == bj (shifted B block on the diagonal), k pair p only for column pairs
+# jp >= p. kb == bi == bj tasks run under FULL. Per NB: the program of each warp slot, or None
+# (every warp FULL, lanes placed freely).
+FULL, DIAG_A, DIAG_B = 0, 1, 2
+ROLES = {8: [FULL, FULL, DIAG_A, DIAG_B]}
+# (iterations, seed) of the lane search where the default (30000, NB) stops short of the best found
+SEARCH = {8: (60000, 8)}
+# largest cell image (chunks) the pad search may produce: the image size fixes the capacity of the
+# allocation-free entry point
+MAX_IMG = {8: 630}
+
 
 def tasks(nb):
     return [(bi, bj, kb) for bi in range(nb) for bj in range(bi, nb) for kb in range(bi, bj + 1)]
+
+
+def role_lanes(nb):
+    """Initial lane order for a role layout: FULL slots take the kb strictly inside (and the
+    kb == bi == bj) tasks, DIAG_A slots the kb == bi < bj tasks, DIAG_B slots the bi < kb == bj."""
+    threads, G = CFG[nb]
+    assert G == 1
+    ts = tasks(nb)
+    pools = {FULL: [t for t in ts if t[0] < t[2] < t[1] or t[0] == t[1]],
+             DIAG_A: [t for t in ts if t[2] == t[0] < t[1]],
+             DIAG_B: [t for t in ts if t[0] < t[2] == t[1]]}
+    lanes, groups = [], []
+    roles = ROLES[nb]
+    for r in set(roles):
+        slots = [w for w, x in enumerate(roles) if x == r]
+        assert len(pools[r]) <= 32 * len(slots), (nb, r)
+    for w, r in enumerate(roles):
+        take = pools[r][:32]
+        pools[r] = pools[r][32:]
+        lanes += [(0, t) for t in take] + [None] * (32 - len(take))
+        groups += [r] * 32
+    assert all(not v for v in pools.values())
+    return lanes, groups
 
 
 class Layout:
@@ -61,17 +97,22 @@ def wavefronts(addrs):
     return max(len(v) for v in groups.values()) if groups else 0
 
 
-def cost(lay, lanes):
+def cost(lay, lanes, groups=None):
     tot = 0
     for qw in range(len(lanes) // 8):
         sel = [x for x in lanes[qw * 8:qw * 8 + 8] if x is not None]
         if not sel:
             continue
+        role = groups[qw * 8] if groups else FULL
         for i in range(8):
             for q in range(2):
+                if role == DIAG_A and q == 0 and i > 4:
+                    continue  # rows 5..7 of k 0..3 are below the subdiagonal
                 tot += wavefronts([lay.a(g, t[0], t[2], i, q) for g, t in sel])
         for k in range(8):
             for h in range(2):
+                if role == DIAG_B and k >= 4 and h == 0:
+                    continue  # columns 0..3 of k 4..7 are below the diagonal
                 tot += wavefronts([lay.b(g, t[2], t[1], k, h) for g, t in sel])
         r3 = [(g, t) for g, t in sel if t[2] == t[0]]
         for h in range(2):
@@ -82,11 +123,15 @@ def cost(lay, lanes):
 def search(nb, iters, seed):
     threads, G = CFG[nb]
     rnd = random.Random(seed)
-    ts = sorted(tasks(nb), key=lambda t: (t[2], t[0], t[1]))
-    lanes = [(g, t) for g in range(G) for t in ts] + [None] * (threads - G * len(ts))
+    if nb in ROLES:
+        lanes, groups = role_lanes(nb)
+    else:
+        ts = sorted(tasks(nb), key=lambda t: (t[2], t[0], t[1]))
+        lanes = [(g, t) for g in range(G) for t in ts] + [None] * (threads - G * len(ts))
+        groups = None
     pads, ipad = [0] * nb, 0
     lay = Layout(nb, pads, ipad)
-    cur = cost(lay, lanes)
+    cur = cost(lay, lanes, groups)
     for _ in range(iters):
         if rnd.random() < 0.2:
             c = rnd.randrange(nb + 1)
@@ -96,17 +141,17 @@ def search(nb, iters, seed):
             else:
                 pads[c] = rnd.randrange(8)
             lay2 = Layout(nb, pads, ipad)
-            cc = cost(lay2, lanes)
-            if cc <= cur:
+            cc = cost(lay2, lanes, groups)
+            if cc <= cur and lay2.img <= MAX_IMG.get(nb, lay2.img):
                 cur, lay = cc, lay2
             else:
                 pads, ipad = old
         else:
             x, y = rnd.randrange(threads), rnd.randrange(threads)
-            if x // 8 == y // 8:
+            if x // 8 == y // 8 or (groups and groups[x] != groups[y]):
                 continue
             lanes[x], lanes[y] = lanes[y], lanes[x]
-            cc = cost(lay, lanes)
+            cc = cost(lay, lanes, groups)
             if cc <= cur:
                 cur = cc
             else:
@@ -119,9 +164,10 @@ def main():
            "// Per inner width class NB = 1..8: threads per CTA, items per iteration, spare chunks after each\n",
            "// block column of a cell image and after each shared-memory item, and lane -> (item slot g, bi,\n",
            "// bj, kb) (0xFF = idle lane).\n"]
-    T, G, P, colpad, colbase, lane_rows = [], [], [], [], [], []
+    T, G, P, colpad, colbase, lane_rows, role_rows = [], [], [], [], [], [], []
     for nb in range(1, 9):
-        c, lanes, pads, ipad = search(nb, 30000, nb)
+        iters, seed = SEARCH.get(nb, (30000, nb))
+        c, lanes, pads, ipad = search(nb, iters, seed)
         threads, g = CFG[nb]
         T.append(threads)
         G.append(g)
@@ -132,6 +178,8 @@ def main():
         rows = ["{255,255,255,255}" if x is None else "{%d,%d,%d,%d}" % (x[0], *x[1])
                 for x in lanes + [None] * (256 - len(lanes))]
         lane_rows.append("{" + ",".join(rows) + "}")
+        roles = ROLES.get(nb, [FULL] * (threads // 32))
+        role_rows.append("{" + ",".join(map(str, roles + [FULL] * (8 - len(roles)))) + "}")
         out.append(f"//   NB={nb}: {threads} threads, {g} items, search cost {c} wavefronts\n")
     out.append("constexpr int R0_TAB_THREADS[9] = {0," + ",".join(map(str, T)) + "};\n")
     out.append("constexpr int R0_TAB_ITEMS[9] = {0," + ",".join(map(str, G)) + "};\n")
@@ -142,6 +190,10 @@ def main():
     out.append("constexpr int R0_TAB_COLBASE[9][9] = " + cbt + ";\n")
     out.append("__constant__ int c_img_colbase[9][9] = " + cbt + ";\n")
     out.append("__constant__ unsigned char c_r0_lane[8][256][4] = {\n" + ",\n".join(lane_rows) + "};\n")
+    out.append("// warp program of each warp slot (0 full task, 1 diagonal A block, 2 diagonal B block)\n")
+    out.append("constexpr unsigned char R0_TAB_ROLE[9][8] = {{0,0,0,0,0,0,0,0}," + ",".join(role_rows) + "};\n")
+    out.append("constexpr bool R0_TAB_HAS_ROLES[9] = {false," +
+               ",".join("true" if nb in ROLES else "false" for nb in range(1, 9)) + "};\n")
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "r0_tables.inc")
     with open(path, "w") as f:
         f.write("".join(out))

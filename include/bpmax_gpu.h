@@ -122,8 +122,9 @@ int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches);
 int bpmax_gpu_profile_kernels(bpmax_ctx *ctx, float *ms, long *launches, double *terms);
 
 /* Measured max-plus issue ceiling of this GPU: a register-resident kernel that runs the
- * instruction mix of the product kernel's inner loop (fp32 add + 3-input max, no memory traffic)
- * on every SM. terms_per_s receives candidates per second. No reference counterpart. */
+ * instruction mix of the product kernel's inner loop (one packed fp32 add making two candidates,
+ * one 3-input max merging them; every candidate a new sum, no memory traffic) on every SM.
+ * terms_per_s receives candidates per second. No reference counterpart. */
 int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s);
 
 /* Score of one pair without allocating any memory. No counterpart in the reference: it serves
@@ -135,7 +136,7 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s);
  * All scratch lives in one fixed 64 MiB device array inside the library, which every GPU that
  * loads the library holds until the process exits. Limits: N <= 64 and, in bytes,
  * T(M)*cell + 4*M^2 + 16*M*ceil(M/2) + (a few KiB) <= 64 MiB, with T(M) = M(M+1)/2 and cell the
- * stored size of one inner table (10080 bytes at N=64, 2912 at N=32, 304 at N<=8): at most
+ * stored size of one inner table (10048 bytes at N=64, 2912 at N=32, 304 at N<=8): at most
  * M=114 for N=64, M=213 for N=32, M=654 for N<=8; larger pairs return BPMAX_EINVAL. The first
  * call on a device looks up the array's device address and sets kernel attributes for that
  * device (make it before any stream capture). Every call reuses the same array, so calls that overlap on the GPU (other threads,
