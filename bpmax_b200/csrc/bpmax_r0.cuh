@@ -33,11 +33,12 @@
 // inside 168 registers without spills). It adds in pairs: (a, a) + (b[j], b[j+1]) with one packed
 // fp32 add (__fadd2_rn, round-to-nearest like the scalar add), and merges four candidates per
 // accumulator with two 3-input max steps.
-// Warp programs (width 64): the lane table groups the tasks by kind, one kind per warp. Tasks
-// with kb == bi < bj (A block on the diagonal) skip the k pairs a row meets only below the
-// subdiagonal, tasks with bi < kb == bj (shifted B block on the diagonal) skip the column pairs a k
-// pair meets only below the diagonal; the skipped candidates are all -inf, so every maximum is
-// unchanged, and those warps issue 92 and 80 of the 128 steps of a full task. At the end of a job the partial maxima of all tasks first meet in a shared
+// Warp programs: the lane table groups the tasks by kind, one program per warp (r0_tables.inc).
+// Tasks with kb == bi (A block on the diagonal) skip the k pairs a row meets only below the
+// subdiagonal, tasks with kb == bj (shifted B block on the diagonal) skip the column pairs a k pair
+// meets only below the diagonal, tasks with both skip both; the skipped candidates are all -inf,
+// so every maximum is unchanged, and those warps issue 92, 80 and 49 of the 128 steps of a full
+// task. At the end of a job the partial maxima of all tasks first meet in a shared
 // tile of the cell's blocks (shared atomicMax; blocks at a pitch of 65 words so the lanes of a
 // warp hit distinct banks), then the tile merges into F(i1, j1) with coalesced global atomicMax,
 // consecutive lanes on consecutive words (max on the int bit patterns is exact: all values are
@@ -89,8 +90,7 @@ struct R0Cfg {
     static constexpr int OFF_CNT = OFF_BAR + 8 * STAGES;  // per stage: warps done with it
     static constexpr size_t SMEM = (size_t)OFF_CNT + 4 * STAGES;
     static constexpr int WARPS = THREADS / 32;
-    // warp program of each warp slot, 2 bits per slot (0 full task, 1 diagonal A, 2 diagonal B)
-    static constexpr bool HAS_ROLES = R0_TAB_HAS_ROLES[NB];
+    // warp program of each warp, 2 bits per warp (0 full task, 1 diagonal A, 2 diagonal B, 3 both)
     static constexpr unsigned ROLE_BITS = R0_TAB_ROLE[NB][0] | R0_TAB_ROLE[NB][1] << 2 | R0_TAB_ROLE[NB][2] << 4 |
                                           R0_TAB_ROLE[NB][3] << 6 | R0_TAB_ROLE[NB][4] << 8 | R0_TAB_ROLE[NB][5] << 10 |
                                           R0_TAB_ROLE[NB][6] << 12 | R0_TAB_ROLE[NB][7] << 14;
@@ -134,11 +134,12 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned
 // ROLE 0 (full) evaluates all 8 k; ROLE 1 (A block on the diagonal, kb == bi) evaluates the k
 // pair p = (2p, 2p+1) only for rows i <= 2p+2, since A[i][k] = -inf for k < i-1; ROLE 2 (shifted B
 // block on the diagonal, kb == bj) evaluates k pair p only for column pairs jp >= p, since
-// Bs[k][j] = -inf for k > j. The skipped candidates are all -inf, so the maxima are unchanged.
+// Bs[k][j] = -inf for k > j; ROLE 3 (both blocks on the diagonal) applies both limits. The
+// skipped candidates are all -inf, so the maxima are unchanged.
 template <int ROLE>
 __device__ __forceinline__ bool r0_pair_used(int i, int jp, int p)
 {
-    return ROLE == 1 ? i <= 2 * p + 2 : (ROLE == 2 ? jp >= p : true);
+    return ((ROLE & 1) == 0 || i <= 2 * p + 2) && ((ROLE & 2) == 0 || jp >= p);
 }
 template <int ROLE>
 __device__ __forceinline__ void r0_task(const float *__restrict__ As, const float *__restrict__ Bs, float (&acc)[8][8])
@@ -219,7 +220,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
     }
 
     // the warp's program (uniform over its lanes) and this thread's task
-    const int role = C::HAS_ROLES ? (int)(C::ROLE_BITS >> (2 * (tid >> 5))) & 3 : 0;
+    const int role = (int)(C::ROLE_BITS >> (2 * (tid >> 5))) & 3;
     const unsigned char *lt = c_r0_lane[NB - 1][tid];
     const bool has_task = lt[0] != 255;
     const int tg = has_task ? lt[0] : 0, bi = lt[1], bj = lt[2], kb = lt[3];
@@ -306,12 +307,14 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         if (active && !bad) {
             const float *item = smem + (size_t)stage * C::STAGE * 4 + tg * C::ITEM * 4;
             const float *As = item + a_off, *Bs = item + b_off;
-            if (!C::HAS_ROLES || role == 0)
+            if (role == 0)
                 r0_task<0>(As, Bs, acc);
             else if (role == 1)
                 r0_task<1>(As, Bs, acc);
-            else
+            else if (role == 2)
                 r0_task<2>(As, Bs, acc);
+            else
+                r0_task<3>(As, Bs, acc);
             if (kb == bi) {  // k = 8bi-1 term of row 8bi: S1(i1,k1) + B[8bi][j2]
                 const float s1a = item[s1_off];
                 const float4 r0 = *reinterpret_cast<const float4 *>(item + r3_off);

@@ -21,51 +21,96 @@ load instruction of the inner loop and of the R3 step.
 """
 from __future__ import annotations
 
+import itertools
 import os
 import random
 
 # (threads per CTA, items per iteration) for each NB: G*TASKS(NB) lanes work, the rest idle
 CFG = {1: (64, 64), 2: (96, 24), 3: (128, 12), 4: (128, 6), 5: (128, 3), 6: (128, 2), 7: (96, 1), 8: (128, 1)}
 
-# Warp programs. FULL: the whole 8x8x8 task. DIAG_A: tasks with kb == bi (A block on the diagonal),
-# k pair (2p, 2p+1) only for rows i <= 2p+2 (the other rows meet -inf below the subdiagonal).
-# DIAG_B: tasks with kb == bj (shifted B block on the diagonal), k pair p only for column pairs
-# jp >= p. kb == bi == bj tasks run under FULL. Per NB: the program of each warp slot, or None
-# (every warp FULL, lanes placed freely).
-FULL, DIAG_A, DIAG_B = 0, 1, 2
-ROLES = {8: [FULL, FULL, DIAG_A, DIAG_B]}
+# Warp programs, one per warp, chosen per lane group from the kinds of its tasks:
+#   FULL     the whole 8x8x8 task (every kind may run under it);
+#   DIAG_A   kb == bi (A block on the diagonal): k pair p = (2p, 2p+1) only for rows i <= 2p+2;
+#   DIAG_B   kb == bj (shifted B block on the diagonal): k pair p only for column pairs jp >= p;
+#   DIAG_AB  kb == bi == bj: both restrictions.
+# A task of kind DD (bi == kb == bj) may run under any program, DA under FULL or DIAG_A, DB under
+# FULL or DIAG_B, F (bi < kb < bj) under FULL only. The cost of a program is its (row, column pair,
+# k pair) steps: 128, 92, 80, 49.
+FULL, DIAG_A, DIAG_B, DIAG_AB = 0, 1, 2, 3
 # (iterations, seed) of the lane search where the default (30000, NB) stops short of the best found
-SEARCH = {8: (60000, 8)}
+SEARCH = {8: (60000, 9)}
 # largest cell image (chunks) the pad search may produce: the image size fixes the capacity of the
 # allocation-free entry point
-MAX_IMG = {8: 630}
+MAX_IMG = {1: 19, 2: 62, 3: 118, 4: 182, 5: 269, 6: 379, 7: 498, 8: 630}
+COST = {FULL: 128, DIAG_A: 92, DIAG_B: 80, DIAG_AB: 49}
+ALLOWED = {FULL: "F DA DB DD", DIAG_A: "DA DD", DIAG_B: "DB DD", DIAG_AB: "DD"}
 
 
 def tasks(nb):
     return [(bi, bj, kb) for bi in range(nb) for bj in range(bi, nb) for kb in range(bi, bj + 1)]
 
 
-def role_lanes(nb):
-    """Initial lane order for a role layout: FULL slots take the kb strictly inside (and the
-    kb == bi == bj) tasks, DIAG_A slots the kb == bi < bj tasks, DIAG_B slots the bi < kb == bj."""
-    threads, G = CFG[nb]
-    assert G == 1
-    ts = tasks(nb)
-    pools = {FULL: [t for t in ts if t[0] < t[2] < t[1] or t[0] == t[1]],
-             DIAG_A: [t for t in ts if t[2] == t[0] < t[1]],
-             DIAG_B: [t for t in ts if t[0] < t[2] == t[1]]}
-    lanes, groups = [], []
-    roles = ROLES[nb]
-    for r in set(roles):
-        slots = [w for w, x in enumerate(roles) if x == r]
-        assert len(pools[r]) <= 32 * len(slots), (nb, r)
+def kind(t):
+    bi, bj, kb = t
+    if bi == bj:
+        return "DD"
+    return "DA" if kb == bi else ("DB" if kb == bj else "F")
+
+
+def pair_used(role, i, jp, p):
+    """Whether a warp running `role` evaluates k pair p for row i and column pair jp."""
+    a = i <= 2 * p + 2
+    b = jp >= p
+    return {FULL: True, DIAG_A: a, DIAG_B: b, DIAG_AB: a and b}[role]
+
+
+def fill(roles, pools):
+    """Places the (item, task) lanes into warps running `roles`: each kind first into the warps of
+    its own program, then into any warp that allows it. None when they do not fit."""
+    pools = {k: list(v) for k, v in pools.items()}
+    warps = [[] for _ in roles]
+    own = {FULL: "F", DIAG_A: "DA", DIAG_B: "DB", DIAG_AB: "DD"}
     for w, r in enumerate(roles):
-        take = pools[r][:32]
-        pools[r] = pools[r][32:]
-        lanes += [(0, t) for t in take] + [None] * (32 - len(take))
+        k = own[r]
+        take = 32 - len(warps[w])
+        warps[w] += pools[k][:take]
+        pools[k] = pools[k][take:]
+    for k in ("F", "DA", "DB", "DD"):
+        for pref in (DIAG_AB, DIAG_A, DIAG_B, FULL):
+            for w, r in enumerate(roles):
+                if r != pref or k not in ALLOWED[r].split():
+                    continue
+                take = 32 - len(warps[w])
+                warps[w] += pools[k][:take]
+                pools[k] = pools[k][take:]
+    if any(pools.values()):
+        return None
+    return warps
+
+
+def role_lanes(nb):
+    """Cheapest warp programs (summed step counts) that hold the G items' tasks, slots ordered
+    FULL, DIAG_A, DIAG_B, DIAG_AB, and the initial lane order."""
+    threads, G = CFG[nb]
+    nw = threads // 32
+    pools = {"F": [], "DA": [], "DB": [], "DD": []}
+    for g in range(G):
+        for t in sorted(tasks(nb), key=lambda t: (t[2], t[0], t[1])):
+            pools[kind(t)].append((g, t))
+    best = None
+    for roles in itertools.combinations_with_replacement((FULL, DIAG_A, DIAG_B, DIAG_AB), nw):
+        warps = fill(list(roles), pools)
+        if warps is None:
+            continue
+        c = sum(COST[r] for r in roles)
+        if best is None or c < best[0]:
+            best = (c, list(roles), warps)
+    _, roles, warps = best
+    lanes, groups = [], []
+    for r, w in zip(roles, warps):
+        lanes += w + [None] * (32 - len(w))
         groups += [r] * 32
-    assert all(not v for v in pools.values())
-    return lanes, groups
+    return lanes, groups, roles
 
 
 class Layout:
@@ -97,22 +142,22 @@ def wavefronts(addrs):
     return max(len(v) for v in groups.values()) if groups else 0
 
 
-def cost(lay, lanes, groups=None):
+def cost(lay, lanes, groups):
     tot = 0
     for qw in range(len(lanes) // 8):
         sel = [x for x in lanes[qw * 8:qw * 8 + 8] if x is not None]
         if not sel:
             continue
-        role = groups[qw * 8] if groups else FULL
+        role = groups[qw * 8]
         for i in range(8):
             for q in range(2):
-                if role == DIAG_A and q == 0 and i > 4:
-                    continue  # rows 5..7 of k 0..3 are below the subdiagonal
+                if not any(pair_used(role, i, 3, p) for p in (2 * q, 2 * q + 1)):
+                    continue  # the program reads no k of this row in this half
                 tot += wavefronts([lay.a(g, t[0], t[2], i, q) for g, t in sel])
         for k in range(8):
             for h in range(2):
-                if role == DIAG_B and k >= 4 and h == 0:
-                    continue  # columns 0..3 of k 4..7 are below the diagonal
+                if h == 0 and not any(pair_used(role, 0, jp, k // 2) for jp in (0, 1)):
+                    continue  # the program reads no column 0..3 of this k
                 tot += wavefronts([lay.b(g, t[2], t[1], k, h) for g, t in sel])
         r3 = [(g, t) for g, t in sel if t[2] == t[0]]
         for h in range(2):
@@ -123,12 +168,7 @@ def cost(lay, lanes, groups=None):
 def search(nb, iters, seed):
     threads, G = CFG[nb]
     rnd = random.Random(seed)
-    if nb in ROLES:
-        lanes, groups = role_lanes(nb)
-    else:
-        ts = sorted(tasks(nb), key=lambda t: (t[2], t[0], t[1]))
-        lanes = [(g, t) for g in range(G) for t in ts] + [None] * (threads - G * len(ts))
-        groups = None
+    lanes, groups, roles = role_lanes(nb)
     pads, ipad = [0] * nb, 0
     lay = Layout(nb, pads, ipad)
     cur = cost(lay, lanes, groups)
@@ -148,7 +188,7 @@ def search(nb, iters, seed):
                 pads, ipad = old
         else:
             x, y = rnd.randrange(threads), rnd.randrange(threads)
-            if x // 8 == y // 8 or (groups and groups[x] != groups[y]):
+            if x // 8 == y // 8 or groups[x] != groups[y]:
                 continue
             lanes[x], lanes[y] = lanes[y], lanes[x]
             cc = cost(lay, lanes, groups)
@@ -156,7 +196,7 @@ def search(nb, iters, seed):
                 cur = cc
             else:
                 lanes[x], lanes[y] = lanes[y], lanes[x]
-    return cur, lanes, pads, ipad
+    return cur, lanes, pads, ipad, roles
 
 
 def main():
@@ -167,7 +207,7 @@ def main():
     T, G, P, colpad, colbase, lane_rows, role_rows = [], [], [], [], [], [], []
     for nb in range(1, 9):
         iters, seed = SEARCH.get(nb, (30000, nb))
-        c, lanes, pads, ipad = search(nb, iters, seed)
+        c, lanes, pads, ipad, roles = search(nb, iters, seed)
         threads, g = CFG[nb]
         T.append(threads)
         G.append(g)
@@ -178,9 +218,8 @@ def main():
         rows = ["{255,255,255,255}" if x is None else "{%d,%d,%d,%d}" % (x[0], *x[1])
                 for x in lanes + [None] * (256 - len(lanes))]
         lane_rows.append("{" + ",".join(rows) + "}")
-        roles = ROLES.get(nb, [FULL] * (threads // 32))
         role_rows.append("{" + ",".join(map(str, roles + [FULL] * (8 - len(roles)))) + "}")
-        out.append(f"//   NB={nb}: {threads} threads, {g} items, search cost {c} wavefronts\n")
+        out.append(f"//   NB={nb}: {threads} threads, {g} items, warp programs {roles}, search cost {c} wavefronts\n")
     out.append("constexpr int R0_TAB_THREADS[9] = {0," + ",".join(map(str, T)) + "};\n")
     out.append("constexpr int R0_TAB_ITEMS[9] = {0," + ",".join(map(str, G)) + "};\n")
     out.append("constexpr int R0_TAB_IPAD[9] = {0," + ",".join(map(str, P)) + "};\n")
@@ -190,10 +229,8 @@ def main():
     out.append("constexpr int R0_TAB_COLBASE[9][9] = " + cbt + ";\n")
     out.append("__constant__ int c_img_colbase[9][9] = " + cbt + ";\n")
     out.append("__constant__ unsigned char c_r0_lane[8][256][4] = {\n" + ",\n".join(lane_rows) + "};\n")
-    out.append("// warp program of each warp slot (0 full task, 1 diagonal A block, 2 diagonal B block)\n")
+    out.append("// warp program of each warp (0 full task, 1 diagonal A block, 2 diagonal B block, 3 both)\n")
     out.append("constexpr unsigned char R0_TAB_ROLE[9][8] = {{0,0,0,0,0,0,0,0}," + ",".join(role_rows) + "};\n")
-    out.append("constexpr bool R0_TAB_HAS_ROLES[9] = {false," +
-               ",".join("true" if nb in ROLES else "false" for nb in range(1, 9)) + "};\n")
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "r0_tables.inc")
     with open(path, "w") as f:
         f.write("".join(out))

@@ -136,8 +136,8 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s);
  * All scratch lives in one fixed 64 MiB device array inside the library, which every GPU that
  * loads the library holds until the process exits. Limits: N <= 64 and, in bytes,
  * T(M)*cell + 4*M^2 + 16*M*ceil(M/2) + (a few KiB) <= 64 MiB, with T(M) = M(M+1)/2 and cell the
- * stored size of one inner table (10048 bytes at N=64, 2912 at N=32, 304 at N<=8): at most
- * M=114 for N=64, M=213 for N=32, M=654 for N<=8; larger pairs return BPMAX_EINVAL. The first
+ * stored size of one inner table (10080 bytes at N=64, 2864 at N=32, 304 at N<=8): at most
+ * M=114 for N=64, M=215 for N=32, M=654 for N<=8; larger pairs return BPMAX_EINVAL. The first
  * call on a device looks up the array's device address and sets kernel attributes for that
  * device (make it before any stream capture). Every call reuses the same array, so calls that overlap on the GPU (other threads,
  * other streams) race and must be serialised by the caller. Errors are returned as status codes

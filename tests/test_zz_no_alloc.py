@@ -34,7 +34,7 @@ def test_noalloc_matches_score_on_two_calls_in_a_row():
 
 
 def test_noalloc_size_limit_is_an_error():
-    s1, s2 = W.pair(115, 64, 13)  # T(115)*10048 bytes of tables + S1 + job lists > 64 MiB
+    s1, s2 = W.pair(115, 64, 13)  # T(115)*10080 bytes of tables + S1 + job lists > 64 MiB
     with pytest.raises(api.BpmaxError) as e:
         api.score_noalloc(s1, s2, W.INTEGER_WEIGHTS)
     assert e.value.status == 1
