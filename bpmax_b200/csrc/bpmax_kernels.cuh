@@ -24,6 +24,7 @@
 //   S1[M][M], S2[Np][Np] single-strand tables (S2 over the reversed strand 2)
 #pragma once
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace bpmax {
@@ -169,6 +170,8 @@ struct FinShape {
     static constexpr int THREADS = NP >= 48 ? 512 : (NP >= 24 ? 256 : 128);
     static constexpr int WARPS = THREADS / 32;
     static constexpr int K = (NP * (NP - 1) / 2 + THREADS - 1) / THREADS;  // owned inner cells per thread
+    static constexpr int MINB = 1536 / THREADS;  // 48 resident warps per SM (at most 40 registers)
+    static_assert(K <= 4, "the step switch covers 4 slots");
     static constexpr size_t SMEM = 2 * (size_t)NP * NP * sizeof(float) + NP;  // D, S2, bases
 };
 
@@ -181,7 +184,7 @@ __device__ __forceinline__ void blk_decode(int NB, int q, int &BI, int &BJ)
 }
 
 template <int NP>
-__global__ void __launch_bounds__(FinShape<NP>::THREADS)
+__global__ void __launch_bounds__(FinShape<NP>::THREADS, FinShape<NP>::MINB)
 finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
                       const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ S,
                       const uint8_t *__restrict__ bases, Weights W, int d)
@@ -238,38 +241,51 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     // (e2, i2): running maxima start at max(accumulated, S1+S2)
     const int ncells = N * (N - 1) / 2;
     int cell_i[K], cell_e[K];
-    float acc[K];
+    float acc[K], sw2[K];  // running maximum; SW2 weight (-inf: no SW2 term)
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         const int c = tid + Sh::THREADS * k;
         cell_e[k] = NP;  // no cell: never open
         cell_i[k] = 0;
         acc[k] = NEG_INF;
+        sw2[k] = NEG_INF;
         if (c < ncells) {
             int e = 1, rem = c;
             while (rem >= N - e) { rem -= N - e; ++e; }
             cell_e[k] = e;
             cell_i[k] = rem;
             acc[k] = fmaxf(img(rem, rem + e), s1v + S2s[rem * NP + rem + e]);
+            if (e >= 4) sw2[k] = score_w(wsh, sb[rem], sb[rem + e]);
         }
     }
     if (tid < N)  // inner diagonal 0
         D[tid] = d == 0 ? score_w(wsh + 6, s1[i1], sb[tid]) : fmaxf(img(tid, tid), s1v + S2s[tid * NP + tid]);
     __syncthreads();
-    for (int e = 0; e + 1 < N; ++e) {
-        const float *De = D + e * NP;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
+    // slot k of every thread holds cells THREADS*k .. THREADS*(k+1)-1 of the (e2, i2) order, so the
+    // slots whose cells are all final (e2 <= e) are the same for every thread: the step enters the
+    // unrolled slot sequence at the first slot still open (a CTA-uniform branch), instead of
+    // evaluating the closed slots under a false predicate
+    auto step = [&](auto kc, int e, const float *De) {
+        constexpr int k = decltype(kc)::value;
+        if constexpr (k < K) {
             const int e2 = cell_e[k];
             if (e2 > e && e2 < NP) {
                 const int i2 = cell_i[k], j2 = i2 + e2;
                 acc[k] = fmax3(acc[k], De[i2] + S2s[(i2 + e + 1) * NP + j2], S2s[i2 * NP + j2 - e - 1] + De[j2 - e]);
-                if (e2 == e + 1) {  // all R1/R2 terms seen: SW2, then the cell is final
-                    float v = acc[k];
-                    if (e2 >= 4) v = fmaxf(v, D[(e2 - 2) * NP + i2 + 1] + score_w(wsh, sb[i2], sb[j2]));
-                    D[e2 * NP + i2] = v;
-                }
+                if (e2 == e + 1)  // all R1/R2 terms seen: SW2, then the cell is final
+                    D[e2 * NP + i2] = fmaxf(acc[k], D[max(e2 - 2, 0) * NP + i2 + 1] + sw2[k]);
             }
+        }
+    };
+    for (int e = 0; e + 1 < N; ++e) {
+        const float *De = D + e * NP;
+        const int first = (e * N - e * (e + 1) / 2) / Sh::THREADS;  // cells with e2 <= e come first
+        switch (first) {
+        case 0: step(std::integral_constant<int, 0>{}, e, De); [[fallthrough]];
+        case 1: step(std::integral_constant<int, 1>{}, e, De); [[fallthrough]];
+        case 2: step(std::integral_constant<int, 2>{}, e, De); [[fallthrough]];
+        case 3: step(std::integral_constant<int, 3>{}, e, De); [[fallthrough]];
+        default: break;
         }
         __syncthreads();
     }
