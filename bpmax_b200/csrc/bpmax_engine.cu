@@ -197,6 +197,8 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         s = align64(s + (long long)pd.Np * pd.Np);
         pd.S2t_off = s;
         s = align64(s + (long long)pd.Np * pd.Np);
+        pd.S2d_off = s;
+        if (pd.Np > MAX_SMALL_NP) s = align64(s + (long long)pd.Np * pd.Np);
         pd.seq1_off = b;
         b += Ms[p];
         pd.seq2_off = b;
@@ -282,6 +284,14 @@ void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 
 void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
+    if (L.np <= FIN_WIDE_MAX_NP) {
+        constexpr int WW = FIN_WIDE_THREADS / 32;
+        finalize_wide_kernel<<<L.count + (L.s1_count + WW - 1) / WW, FIN_WIDE_THREADS, fin_wide_smem(L.np), s>>>(
+            (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first,
+            L.s1_count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
+            (const uint8_t *)ctx->bases.p, ctx->W, L.d);
+        return;
+    }
     constexpr int W = FIN_LARGE_THREADS / 32;
     finalize_large_kernel<<<L.count + (L.s1_count + W - 1) / W, FIN_LARGE_THREADS, 0, s>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
@@ -316,8 +326,11 @@ int set_smem_attr(bpmax_ctx *ctx)
     CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)FinShape<8 * NB>::SMEM));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ[NB], r0_kernel<NB>, R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM));
-    if (NB == 8)
+    if (NB == 8) {
         CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideShape::SMEM));
+        CK(cudaFuncSetAttribute(finalize_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fin_wide_smem(FIN_WIDE_MAX_NP)));
+    }
     return BPMAX_OK;
 }
 

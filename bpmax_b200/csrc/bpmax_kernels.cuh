@@ -51,6 +51,7 @@ struct PairDesc {
     long long S2_off;  // float offset of S2 in the S arena
     long long S2m_off; // Np > 64 only: S2 with -inf outside its triangle
     long long S2t_off; // Np > 64 only: ST1[j][k] = S2(k+1, j), -inf outside
+    long long S2d_off; // Np > 64 only: S2 diagonal-major, S2D[e][i] = S2(i, i+e), -inf outside
     int seq1_off;      // offset of seq1 in the base arena (uint8)
     int seq2_off;      // offset of the REVERSED seq2 in the base arena (uint8)
 };
@@ -174,6 +175,9 @@ struct FinShape {
     static_assert(K <= 4, "the step switch covers 4 slots");
     static constexpr size_t SMEM = 2 * (size_t)NP * NP * sizeof(float) + NP;  // D, S2, bases
 };
+
+// first float of row e of a triangular diagonal-major table of width NP (row e holds NP - e entries)
+__host__ __device__ __forceinline__ int drow(int NP, int e) { return e * NP - e * (e - 1) / 2; }
 
 // (BI, BJ) of the q-th block of the upper block triangle (row-major triangle order)
 __device__ __forceinline__ void blk_decode(int NB, int q, int &BI, int &BJ)

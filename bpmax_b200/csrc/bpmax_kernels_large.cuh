@@ -60,20 +60,24 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 
 // ------------------------------------------------------------------------------------------
-// Masked copies of S2: S2M[i][k] = S2(i,k) if i <= k < N else -inf and
-// ST1[j][k] = S2(k+1,j) if k+1 <= j < N else -inf (S2 over the reversed strand 2,
-// V3/bpmax_verify.c:560-571), read by the inner wavefront of every width. One CTA per pair.
+// Rearranged copies of S2 (S2 over the reversed strand 2, V3/bpmax_verify.c:560-571) for the wide
+// inner wavefronts (Np > 64): the masked S2M[i][k] = S2(i,k) if i <= k < N else -inf and
+// ST1[j][k] = S2(k+1,j) if k+1 <= j < N else -inf (global-memory wavefront), and the
+// diagonal-major S2D[e][i] = S2(i, i+e) if i+e < N else -inf (shared-memory wavefront). One CTA
+// per pair; pairs of the cell-image widths have nothing to do.
 // ------------------------------------------------------------------------------------------
 __global__ void s2_aux_kernel(const PairDesc *__restrict__ pairs, float *__restrict__ S)
 {
     const PairDesc pd = pairs[blockIdx.x];
     const int Np = pd.Np, N = pd.N;
+    if (Np <= 64) return;
     const float *S2 = S + pd.S2_off;
-    float *S2M = S + pd.S2m_off, *ST1 = S + pd.S2t_off;
+    float *S2M = S + pd.S2m_off, *ST1 = S + pd.S2t_off, *S2D = S + pd.S2d_off;
     for (int q = threadIdx.x; q < Np * Np; q += blockDim.x) {
         const int r = q / Np, c = q % Np;
         S2M[q] = (r <= c && c < N) ? S2[q] : NEG_INF;
         ST1[q] = (c + 1 <= r && r < N) ? S2[(c + 1) * Np + r] : NEG_INF;
+        S2D[q] = c + r < N ? S2[c * Np + c + r] : NEG_INF;  // r = e, c = i
     }
 }
 
@@ -358,6 +362,106 @@ finalize_large_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
     for (int r = 1 + tid; r < Np; r += NT) {
         Fc[(long long)r * Np + r - 1] = s1v;
         FTc[(long long)(r - 1) * Np + r] = s1v;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Finalize for 64 < Np <= FIN_WIDE_MAX_NP: same candidates and same results as
+// finalize_large_kernel, with the inner wavefront pushed forward in shared memory. The CTA keeps
+// the cell's inner table diagonal-major and triangular, D[e][i2] = F[i2][i2+e] (T(Np) floats),
+// each open entry holding its running maximum. When inner diagonal e is final, every open cell
+// (e2 > e) takes its two candidates that read diagonal e,
+//   R1 with k2 = i2+e:    F[i2][i2+e] + S2(i2+e+1, j2)
+//   R2 with k2 = j2-e-1:  S2(i2, j2-e-1) + F[j2-e][j2]
+// and the cells of diagonal e+1 become final after SW2. Warp w takes the diagonals e2 = e+1+w,
+// e+1+w+32, ...; its lanes take consecutive i2, so both S2 reads are one coalesced line of the
+// diagonal-major copy and the D reads are conflict-free. One CTA barrier per inner diagonal. F
+// and FT are written once, at the end, row by row.
+// CTAs after the first njobs compute S1 on diagonal d+1, one warp per cell.
+// ------------------------------------------------------------------------------------------
+constexpr int FIN_WIDE_THREADS = 1024;
+constexpr int FIN_WIDE_MAX_NP = 320;  // T(320) floats = 205,440 bytes of shared memory
+
+__host__ __device__ constexpr size_t fin_wide_smem(int Np) { return (size_t)Np * (Np + 1) / 2 * 4 + Np; }
+
+__global__ void __launch_bounds__(FIN_WIDE_THREADS)
+finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
+                     const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
+                     float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
+{
+    constexpr int NT = FIN_WIDE_THREADS, WARPS = NT / 32;
+    extern __shared__ __align__(16) float fwd[];
+    __shared__ float wsh[12];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < 12) wsh[tid] = W.w[tid];
+    __syncthreads();
+    if ((int)blockIdx.x >= njobs) {  // S1 cells (i, i+d+1), one per warp
+        const int q = ((int)blockIdx.x - njobs) * WARPS + warp;
+        if (q >= ns1) return;
+        const CellJob job = s1jobs[q];
+        const PairDesc pd = pairs[job.pair];
+        const int M = pd.M, i = job.i1, j = i + d + 1;
+        float *S1 = S + pd.S1_off;
+        if (j - i <= 3) return;
+        const uint8_t *s1 = bases + pd.seq1_off;
+        float red = NEG_INF;
+        for (int k = i + lane; k < j; k += 32) red = fmaxf(red, S1[i * M + k] + S1[(k + 1) * M + j]);
+        for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
+        if (lane == 0) S1[i * M + j] = fmaxf(S1[(i + 1) * M + (j - 1)] + score_w(wsh, s1[i], s1[j]), red);
+        return;
+    }
+    const CellJob job = jobs[blockIdx.x];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1, j1 = i1 + d;
+    const long long tile = (long long)Np * Np;
+    float *Fc = F + pd.F_off + cell_index(M, i1, j1) * tile;
+    float *FTc = FT + pd.F_off + cell_index(M, i1, j1) * tile;
+    const float *S1 = S + pd.S1_off;
+    const float *S2 = S + pd.S2_off;
+    const float *S2D = S + pd.S2d_off;
+    const uint8_t *s1 = bases + pd.seq1_off;
+    float *D = fwd;
+    uint8_t *sb = reinterpret_cast<uint8_t *>(fwd + Np * (Np + 1) / 2);
+    for (int r = tid; r < Np; r += NT) sb[r] = r < N ? bases[pd.seq2_off + r] : 4;
+    const float s1v = S1[i1 * M + j1];
+    __syncthreads();
+    // start values: max(accumulated, S1+S2), or the inter-strand base on the diagonal of the
+    // diagonal cells
+    for (int q = tid; q < Np * Np; q += NT) {
+        const int r = q / Np, c = q % Np;
+        if (r <= c && c < N)
+            D[drow(Np, c - r) + r] = (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(Fc[q], s1v + S2[q]);
+    }
+    __syncthreads();
+    for (int e = 0; e + 1 < N; ++e) {
+        const float *De = D + drow(Np, e);
+        for (int e2 = e + 1 + warp; e2 < N; e2 += WARPS) {
+            float *Dw = D + drow(Np, e2);
+            const float *S2r = S2D + (long long)(e2 - e - 1) * Np;
+            const bool fin = e2 == e + 1 && e2 >= 4;  // SW2 when the cell becomes final
+            const float *Dp = D + drow(Np, max(e2 - 2, 0)) + 1;
+            for (int i2 = lane; i2 < N - e2; i2 += 32) {
+                const int j2 = i2 + e2;
+                float v = fmax3(Dw[i2], De[i2] + S2r[i2 + e + 1], S2r[i2] + De[j2 - e]);
+                if (fin) v = fmaxf(v, Dp[i2] + score_w(wsh, sb[i2], sb[j2]));
+                Dw[i2] = v;
+            }
+        }
+        __syncthreads();
+    }
+    // F and FT, row by row: the logical triangle, S1(i1,j1) on the subdiagonal, -inf elsewhere;
+    // SW1 candidate of cell (i1-1, j1+1), whose table nothing else has written yet
+    const bool push = i1 >= 1 && j1 + 1 < M && d + 2 >= 4;
+    const float wp = push ? score_w(wsh, s1[i1 - 1], s1[j1 + 1]) : 0.0f;
+    float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * tile : nullptr;
+    for (int q = tid; q < Np * Np; q += NT) {
+        const int r = q / Np, c = q % Np;
+        const bool vf = r <= c && c < N, vt = c <= r && r < N;
+        const float f = vf ? D[drow(Np, c - r) + r] : (r == c + 1 ? s1v : NEG_INF);
+        const float t = vt ? D[drow(Np, r - c) + c] : (c == r + 1 ? s1v : NEG_INF);  // F[c][r]
+        Fc[q] = f;
+        FTc[q] = t;
+        if (push) Fn[q] = vf ? f + wp : 0.0f;
     }
 }
 
