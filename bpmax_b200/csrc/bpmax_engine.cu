@@ -309,14 +309,23 @@ void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
                                                               (int *)ctx->errflag.p);
 }
 
-template <int NB>
-void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
+template <int NB, int T>
+void launch_fin_t(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
-    using Sh = FinShape<8 * NB>;
-    finalize_small_kernel<8 * NB><<<L.count + (L.s1_count + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
+    using Sh = FinShape<8 * NB, T>;
+    finalize_small_kernel<8 * NB, T><<<L.count + (L.s1_count + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
         (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W,
         L.d);
+}
+
+template <int NB>
+void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
+{
+    if constexpr (8 * NB >= 48) {
+        if (L.count >= FIN_BULK_CELLS) return launch_fin_t<NB, FIN_BULK_THREADS>(ctx, L, s);
+    }
+    launch_fin_t<NB, fin_threads(8 * NB)>(ctx, L, s);
 }
 
 template <int NB>
@@ -325,6 +334,9 @@ int set_smem_attr(bpmax_ctx *ctx)
     CK(cudaFuncSetAttribute(r0_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM));
     CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)FinShape<8 * NB>::SMEM));
+    if constexpr (8 * NB >= 48)
+        CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB, FIN_BULK_THREADS>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FinShape<8 * NB, FIN_BULK_THREADS>::SMEM));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ[NB], r0_kernel<NB>, R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM));
     if (NB == 8) {
         CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideShape::SMEM));

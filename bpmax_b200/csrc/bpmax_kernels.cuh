@@ -165,14 +165,20 @@ struct CellJob {
     int pair, i1;
 };
 
-template <int NP>
+// threads per cell: the wavefront's serial work per step is K owned cells per thread. Fewer
+// threads per cell cost latency per cell but issue fewer instructions per step in total, which pays
+// when a launch holds many more cells than the GPU runs at once (FIN_WIDE_CELLS below)
+constexpr int fin_threads(int NP) { return NP >= 48 ? 512 : (NP >= 24 ? 256 : 64); }
+constexpr int FIN_BULK_THREADS = 256;  // widths >= 48, launches of FIN_BULK_CELLS cells or more
+constexpr int FIN_BULK_CELLS = 2048;
+
+template <int NP, int T = fin_threads(NP)>
 struct FinShape {
-    // threads per cell: the wavefront's serial work per step is K owned cells per thread
-    static constexpr int THREADS = NP >= 48 ? 512 : (NP >= 24 ? 256 : 128);
+    static constexpr int THREADS = T;
     static constexpr int WARPS = THREADS / 32;
     static constexpr int K = (NP * (NP - 1) / 2 + THREADS - 1) / THREADS;  // owned inner cells per thread
     static constexpr int MINB = 1536 / THREADS;  // 48 resident warps per SM (at most 40 registers)
-    static_assert(K <= 4, "the step switch covers 4 slots");
+    static_assert(K <= 8, "the step switch covers 8 slots");
     static constexpr size_t SMEM = 2 * (size_t)NP * NP * sizeof(float) + NP;  // D, S2, bases
 };
 
@@ -187,13 +193,13 @@ __device__ __forceinline__ void blk_decode(int NB, int q, int &BI, int &BJ)
     BJ = BI + q;
 }
 
-template <int NP>
-__global__ void __launch_bounds__(FinShape<NP>::THREADS, FinShape<NP>::MINB)
+template <int NP, int T = fin_threads(NP)>
+__global__ void __launch_bounds__(FinShape<NP, T>::THREADS, FinShape<NP, T>::MINB)
 finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
                       const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ S,
                       const uint8_t *__restrict__ bases, Weights W, int d)
 {
-    using Sh = FinShape<NP>;
+    using Sh = FinShape<NP, T>;
     constexpr int NB = NP / 8, NBLK = NB * (NB + 1) / 2, K = Sh::K;
     constexpr long long CELL = 4LL * R0_TAB_COLBASE[NB][NB];
     extern __shared__ __align__(16) float fsm[];
@@ -289,6 +295,10 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
         case 1: step(std::integral_constant<int, 1>{}, e, De); [[fallthrough]];
         case 2: step(std::integral_constant<int, 2>{}, e, De); [[fallthrough]];
         case 3: step(std::integral_constant<int, 3>{}, e, De); [[fallthrough]];
+        case 4: step(std::integral_constant<int, 4>{}, e, De); [[fallthrough]];
+        case 5: step(std::integral_constant<int, 5>{}, e, De); [[fallthrough]];
+        case 6: step(std::integral_constant<int, 6>{}, e, De); [[fallthrough]];
+        case 7: step(std::integral_constant<int, 7>{}, e, De); [[fallthrough]];
         default: break;
         }
         __syncthreads();
