@@ -87,6 +87,19 @@ def test_batched_uneven_matches_oracle_and_each(eng, oracle_mod):
     assert np.array_equal(bits(each), bits(exp))
 
 
+def test_batched_bulk_finalize_matches_oracle(eng, oracle_mod):
+    # 128 pairs of width class 64: the finalize launches of the first outer diagonals hold 2,048 or
+    # more cells and take the 256-thread form, the later ones the 512-thread form
+    rng = np.random.default_rng(91)
+    pairs = [(W.random_sequence(20, rng), W.random_sequence(int(rng.integers(57, 65)), rng)) for _ in range(128)]
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    got = eng.score_batch(pairs)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
+                   dtype=np.float32)
+    assert np.array_equal(bits(got), bits(exp))
+    assert np.array_equal(bits(eng.score_each(pairs)), bits(exp))
+
+
 def test_repeated_calls_and_shape_changes(eng, oracle_mod):
     eng.set_weights(W.INTEGER_WEIGHTS)
     for (M, N, seed) in [(12, 20, 31), (12, 20, 32), (6, 44, 33), (12, 20, 31)]:
