@@ -325,3 +325,34 @@ int oracle_reference_written(long M, long N, long T, long idx)
     if (r < T && r < Ri) return 0;
     return 1;
 }
+
+int oracle_r0only(long M, long N, const int *seq1, const int *seq2, float *F)
+{
+    if (M < 1 || N < 1) return -1;
+    const long NN = N * N;
+    for (long d1 = 0; d1 < M; ++d1)
+        for (long i1 = 0; i1 + d1 < M; ++i1) {
+            const long j1 = i1 + d1;
+            float *C = F + oracle_cell(M, i1, j1) * NN;
+            for (long q = 0; q < NN; ++q) C[q] = -FLT_MAX;
+            for (long d2 = 0; d2 < N; ++d2)
+                for (long i2 = 0; i2 + d2 < N; ++i2) {
+                    const long j2 = i2 + d2;
+                    float v;
+                    if (j1 == i1) {
+                        v = (float)seq2[i2];
+                    } else if (j2 == i2) {
+                        v = (float)seq1[i1];
+                    } else {
+                        v = -INFINITY;
+                        for (long k1 = i1; k1 < j1; ++k1) {
+                            const float *A = F + oracle_cell(M, i1, k1) * NN;
+                            const float *B = F + oracle_cell(M, k1 + 1, j1) * NN;
+                            for (long k2 = i2; k2 < j2; ++k2) v = max_r(v, A[i2 * N + k2] + B[(k2 + 1) * N + j2]);
+                        }
+                    }
+                    C[i2 * N + j2] = v;
+                }
+        }
+    return 0;
+}

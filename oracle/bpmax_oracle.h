@@ -75,6 +75,16 @@ void oracle_to_reference_layout(long M, long N, long N_tile, const float *F, flo
 /* 1 if reference-layout cell (linear index idx) is one the reference fill writes, else 0. */
 int oracle_reference_written(long M, long N, long N_tile, long idx);
 
+/* R0-only double max-plus (the IPDPSW microbenchmark spec,
+ * IPDPSW/source/R0/ospsq_coarse_diag_top_down/ospsq_float.ab:1-15; its C kernel is
+ * IPDPSW/source/R0/ospsq_coarse_diag_top_down/src/ospsqmax_float.c:113-189):
+ *   F(i1,i1,i2,j2) = seq2[i2]
+ *   F(i1,j1,i2,i2) = seq1[i1]                                            (j1 > i1)
+ *   F(i1,j1,i2,j2) = max_{i1<=k1<j1, i2<=k2<j2} F(i1,k1,i2,k2) + F(k1+1,j1,k2+1,j2)   (j1 > i1, j2 > i2)
+ * with the integer sequences converted to float. F: compact layout as oracle_fill (T(M) cells
+ * of N x N, -FLT_MAX where i2 > j2). Returns 0, or -1 for M < 1 or N < 1. */
+int oracle_r0only(long M, long N, const int *seq1, const int *seq2, float *F);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,6 +23,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _ORACLE = os.path.join(HERE, "liboracle.so")
 _REF = os.path.join(HERE, "_ref", "libbpmax_ref.so")
+_REF_R0_CHECK = os.path.join(HERE, "_ref", "ospsqmax_check")  # the reference's R0-only program, printing F
+_REF_R0_TIME = os.path.join(HERE, "_ref", "ospsqmax_time")    # the same, random sequences, timing only
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -55,6 +57,8 @@ def lib():
         L.oracle_reference_size.restype = ctypes.c_long
         L.oracle_single_strand.argtypes = [_L, _i32p, _f32p, _f32p]
         L.oracle_single_strand.restype = None
+        L.oracle_r0only.argtypes = [_L, _L, _i32p, _i32p, _f32p]
+        L.oracle_r0only.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -98,6 +102,45 @@ def fill(seq1, seq2, w12):
     if rc != 0:
         raise ValueError("oracle_fill rejected its arguments")
     return F, S1, S2
+
+
+def r0only(seq1, seq2):
+    """R0-only double max-plus (oracle_r0only). seq1, seq2: non-negative integer sequences.
+    Returns F[T(M), N, N] (compact layout, -FLT_MAX where i2 > j2)."""
+    s1 = np.ascontiguousarray(seq1, dtype=np.int32)
+    s2 = np.ascontiguousarray(seq2, dtype=np.int32)
+    M, N = len(s1), len(s2)
+    F = np.empty((M * (M + 1) // 2, N, N), dtype=np.float32)
+    if lib().oracle_r0only(M, N, s1, s2, F) != 0:
+        raise ValueError("oracle_r0only rejected its arguments")
+    return F
+
+
+def ref_r0only_available() -> bool:
+    return os.path.exists(_REF_R0_CHECK)
+
+
+def ref_r0only(seq1, seq2):
+    """The reference's own R0-only program (oracle/_ref/ospsqmax_check, built from
+    IPDPSW/source/R0/ospsq_coarse_diag_top_down/src by oracle/Makefile with -DCHECKING
+    -DNO_PROMPT): sequences on stdin, every F(i1<=j1, i2<=j2) printed with %0.2f. Returns the
+    compact F like r0only (exact: the printed values are integers)."""
+    s1 = [int(x) for x in seq1]
+    s2 = [int(x) for x in seq2]
+    M, N = len(s1), len(s2)
+    out = subprocess.run([_REF_R0_CHECK, str(M), str(N)], input=" ".join(map(str, s1 + s2)) + "\n",
+                         capture_output=True, text=True, check=True, env=dict(os.environ, OMP_NUM_THREADS="1"))
+    lines = out.stdout.splitlines()
+    vals = [float(x) for x in lines[lines.index(next(l for l in lines if l.startswith("Execution time"))) + 1:]]
+    F = np.full((M * (M + 1) // 2, N, N), -np.finfo(np.float32).max, dtype=np.float32)
+    it = iter(vals)
+    for i1 in range(M):
+        for j1 in range(i1, M):
+            c = cell(M, i1, j1)
+            for i2 in range(N):
+                for j2 in range(i2, N):
+                    F[c, i2, j2] = next(it)
+    return F
 
 
 def cell(M: int, i1: int, j1: int) -> int:

@@ -1,5 +1,8 @@
 """The oracle (CPU restatement of bpmax_verify.c) against the reference's golden fixtures and,
 where the reference was built here, against the reference's own programs."""
+import hashlib
+import os
+
 import numpy as np
 import pytest
 
@@ -81,3 +84,32 @@ def test_traceback_counts_match_finite_differences(oracle_mod):
             assert abs(fd - c[t]) < 0.05
             checked += 1
     assert checked >= 24
+
+
+R0_GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "r0only.npz")
+
+
+def _r0_cases():
+    z = np.load(R0_GOLDEN)
+    names = sorted({k.split("/")[0] for k in z.files})
+    return [(n, z[f"{n}/seq1"], z[f"{n}/seq2"], str(z[f"{n}/sha"]), z[f"{n}/F"] if f"{n}/F" in z.files else None)
+            for n in names]
+
+
+@pytest.mark.parametrize("case", _r0_cases(), ids=lambda c: c[0])
+def test_r0only_oracle_matches_reference_golden(oracle_mod, case):
+    """The R0-only restatement against tables the reference's own ospsqmax program printed."""
+    name, s1, s2, digest, F = case
+    got = oracle_mod.r0only(s1, s2)
+    assert hashlib.sha256(got.tobytes()).hexdigest() == digest
+    if F is not None:
+        assert np.array_equal(got.view(np.uint32), F.view(np.uint32))
+
+
+def test_r0only_oracle_matches_reference_program(oracle_mod):
+    if not oracle_mod.ref_r0only_available():
+        pytest.skip("the reference's R0-only program is not built here")
+    rng = np.random.default_rng(17)
+    for M, N in [(3, 5), (6, 9), (4, 17)]:
+        s1, s2 = rng.integers(0, 2**31 - 1, M), rng.integers(0, 2**31 - 1, N)
+        assert np.array_equal(oracle_mod.r0only(s1, s2).view(np.uint32), oracle_mod.ref_r0only(s1, s2).view(np.uint32))
