@@ -57,6 +57,7 @@ def load_library():
     L.bpmax_gpu_set_weights.argtypes = [vp, vp]
     L.bpmax_gpu_fill.argtypes = [vp, vp, c_long, vp, c_long, c_long, vp, vp]
     L.bpmax_gpu_fill_compact.argtypes = [vp, vp, c_long, vp, c_long, vp, vp]
+    L.bpmax_gpu_r0_only.argtypes = [vp, vp, c_long, vp, c_long, vp, vp]
     L.bpmax_gpu_score.argtypes = [vp, vp, c_long, vp, c_long, vp]
     for name in ("bpmax_gpu_score_batch", "bpmax_gpu_score_each"):
         getattr(L, name).argtypes = [vp, c_int, vp, vp, vp, vp, vp]
@@ -145,6 +146,18 @@ class Engine:
         F = np.empty((M * (M + 1) // 2, N, N), dtype=np.float32)
         sc = np.zeros(1, dtype=np.float32)
         self._check(self._L.bpmax_gpu_fill_compact(self._ctx, _ptr(a), M, _ptr(b), N, _ptr(F), _ptr(sc)))
+        return F, float(sc[0])
+
+    def r0_only(self, seq1, seq2, want_table: bool = True):
+        """bpmax_gpu_r0_only: the R0-only double max-plus microbenchmark of the reference's IPDPSW
+        program (non-negative integer sequences). Returns (F[T(M), N, N] float32 or None, score)."""
+        a = np.ascontiguousarray(seq1, dtype=np.int32)
+        b = np.ascontiguousarray(seq2, dtype=np.int32)
+        M, N = len(a), len(b)
+        F = np.empty((M * (M + 1) // 2, N, N), dtype=np.float32) if want_table else None
+        sc = np.zeros(1, dtype=np.float32)
+        self._check(self._L.bpmax_gpu_r0_only(self._ctx, _ptr(a), M, _ptr(b), N, _ptr(F) if want_table else None,
+                                              _ptr(sc)))
         return F, float(sc[0])
 
     @staticmethod

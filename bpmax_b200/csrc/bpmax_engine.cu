@@ -27,6 +27,7 @@
 #include "bpmax_kernels_large.cuh"
 #include "bpmax_r0.cuh"
 #include "bpmax_adjoint.cuh"
+#include "bpmax_r0only.cuh"
 
 using namespace bpmax;
 
@@ -79,6 +80,7 @@ struct Plan {
     std::vector<CellJob> cell_jobs;
     std::vector<int> classes;  // distinct inner widths, ascending
     int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
+    bool r0_only = false;  // R0-only double max-plus (bpmax_gpu_r0_only) instead of the BPMax fill
     std::vector<cudaEvent_t> diag_ev;  // one pair only: outer diagonal d finalized (recorded by the graph)
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
@@ -97,6 +99,8 @@ struct bpmax_ctx {
     Weights W;
     std::string err;
     DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
+    DevBuf r0vals;         // R0-only mode: seq1 then seq2 of the pair, as floats
+    bool r0_only = false;  // mode of the next prepare()
     int r0_occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class NB
     // schedule tunables (bpmax_gpu_set_tuning / bpmax_gpu_autotune); a plan is built with the
     // values current at build time, or with the values an autotune run stored for its shapes
@@ -328,6 +332,26 @@ void launch_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     launch_fin_t<NB, fin_threads(8 * NB)>(ctx, L, s);
 }
 
+void launch_r0only_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
+{
+    const CellJob *jobs = (const CellJob *)ctx->celljobs.p + L.first;
+    const PairDesc *pd = (const PairDesc *)ctx->pairs.p;
+    const float *vals = (const float *)ctx->r0vals.p;
+    switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
+    case 0:
+        r0only_finalize_wide_kernel<<<L.count, 512, 0, s>>>(jobs, pd, (float *)ctx->F.p, (float *)ctx->FT.p, vals, L.d);
+        break;
+    case 1: r0only_finalize_small_kernel<8><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    case 2: r0only_finalize_small_kernel<16><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    case 3: r0only_finalize_small_kernel<24><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    case 4: r0only_finalize_small_kernel<32><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    case 5: r0only_finalize_small_kernel<40><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    case 6: r0only_finalize_small_kernel<48><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    case 7: r0only_finalize_small_kernel<56><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    default: r0only_finalize_small_kernel<64><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
+    }
+}
+
 template <int NB>
 int set_smem_attr(bpmax_ctx *ctx)
 {
@@ -381,13 +405,17 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
     CK(cudaMemsetAsync(ctx->F.p, 0, (size_t)P.F_floats * sizeof(float), ctx->stream));
     CK(cudaMemsetAsync(ctx->S.p, 0, (size_t)P.S_floats * sizeof(float), ctx->stream));  // S1 starts at 0
     CK(cudaMemsetAsync(ctx->errflag.p, 0, sizeof(int), ctx->stream));
-    {
+    if (P.r0_only) {
+        ProfScope ps(ctx, kp, 0);
+        r0only_prep_kernel<<<(int)P.pairs.size(), 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (float *)ctx->S.p);
+        launches += 1;
+    } else {
         ProfScope ps(ctx, kp, 0);
         single_strand_kernel<<<(int)P.pairs.size(), 512, 0, ctx->stream>>>(
             (const PairDesc *)ctx->pairs.p, (const uint8_t *)ctx->bases.p, (float *)ctx->S.p, ctx->W);
         s2_aux_kernel<<<(int)P.pairs.size(), 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (float *)ctx->S.p);
+        launches += 2;
     }
-    launches += 2;
     // pairs of different inner widths never interact: each width class runs its own chain of
     // diagonals on its own stream (parallel branches of the captured graph); profiling runs
     // serialise everything on the main stream so every launch can be timed
@@ -424,6 +452,10 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
             const auto &L = P.fin_launches[fi];
             const cudaStream_t st = stream_of(L.np);
             ProfScope ps(ctx, kp, 2);
+            if (P.r0_only) {
+                launch_r0only_fin(ctx, L, st);
+                continue;
+            }
             switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
             case 0: launch_fin_large(ctx, L, st); break;
             case 1: launch_fin<1>(ctx, L, st); break;
@@ -461,7 +493,7 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
                                         : std::array<int, 3>{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams};
     const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
                              ctx->plan.class_streams == want[2];
-    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning)) {
+    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
         ctx->plan.graph = nullptr;
         for (cudaEvent_t e : ctx->plan.diag_ev) cudaEventDestroy(e);
@@ -469,6 +501,7 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
         ctx->plan_valid = false;
         if ((st = build_plan(ctx, Ms, Ns, ctx->plan)) != BPMAX_OK) return st;
         Plan &P = ctx->plan;
+        P.r0_only = ctx->r0_only;
         if (P.pairs.size() == 1) {
             P.diag_ev.assign(P.maxM, nullptr);
             for (auto &e : P.diag_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -493,8 +526,17 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->plan_valid = true;
     }
-    // sequences: seq1 as is, seq2 reversed (V3/transform_reverse_1D_to_2D.c:131-135)
     Plan &P = ctx->plan;
+    if (P.r0_only) {  // the sequences are the base values themselves: seq1, then seq2 unreversed
+        std::vector<float> hv;
+        for (int i = 0; i < Ms[0]; ++i) hv.push_back((float)s1s[0][i]);
+        for (int i = 0; i < Ns[0]; ++i) hv.push_back((float)s2s[0][i]);
+        if ((st = ensure(ctx, ctx->r0vals, hv.size() * sizeof(float))) != BPMAX_OK) return st;
+        CK(cudaMemcpyAsync(ctx->r0vals.p, hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return BPMAX_OK;
+    }
+    // sequences: seq1 as is, seq2 reversed (V3/transform_reverse_1D_to_2D.c:131-135)
     std::vector<uint8_t> hb(P.bases_bytes);
     for (size_t p = 0; p < P.pairs.size(); ++p) {
         const PairDesc &pd = P.pairs[p];
@@ -755,6 +797,36 @@ int bpmax_gpu_score_each(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s,
     return BPMAX_OK;
 }
 
+int bpmax_gpu_r0_only(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *F_compact,
+                      float *score)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (!seq1 || !seq2) return fail(ctx, BPMAX_EINVAL, "null sequence");
+    // the reference's domain {M,N | M>=2 && N>=2} (IPDPSW/.../ospsq_float.ab:1)
+    if (M < 2 || N < 2 || M > 65535) return fail(ctx, BPMAX_EINVAL, "The value of parameters are not valid.");
+    if (padded_width((int)N) > MAX_NP) return fail(ctx, BPMAX_EINVAL, "strand-2 length %ld > %d is not supported", N, MAX_NP);
+    for (long i = 0; i < M; ++i)
+        if (seq1[i] < 0) return fail(ctx, BPMAX_EINVAL, "seq1[%ld] = %d < 0: values must be non-negative", i, seq1[i]);
+    for (long i = 0; i < N; ++i)
+        if (seq2[i] < 0) return fail(ctx, BPMAX_EINVAL, "seq2[%ld] = %d < 0: values must be non-negative", i, seq2[i]);
+    CK(cudaSetDevice(ctx->device));
+    ctx->r0_only = true;
+    int st = prepare(ctx, {(int)M}, {(int)N}, {seq1}, {seq2});
+    ctx->r0_only = false;
+    if (st) return st;
+    if ((st = run_fill(ctx)) != BPMAX_OK) return st;
+    if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+    if (!F_compact) return BPMAX_OK;
+    const long long n_out = M * (M + 1) / 2 * N * N;
+    if ((st = ensure(ctx, ctx->conv, n_out * sizeof(float))) != BPMAX_OK) return st;
+    to_compact_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p,
+                                                             n_out, (float *)ctx->conv.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(F_compact, ctx->conv.p, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BPMAX_OK;
+}
+
 int bpmax_gpu_fill_compact(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *F_compact,
                            float *score)
 {
@@ -886,6 +958,10 @@ int bpmax_gpu_profile_kernels(bpmax_ctx *ctx, float *ms, long *launches, double 
     auto T = [](double n) { return n * (n + 1) / 2.0; };
     double t[3] = {0, 0, 0};
     for (const PairDesc &pd : ctx->plan.pairs) {
+        if (ctx->plan.r0_only) {  // the double max-plus alone; the other kinds only place values
+            t[1] += C(pd.M) * C(pd.N);
+            continue;
+        }
         t[0] += C(pd.M) + C(pd.N);
         t[1] += C(pd.M) * (C(pd.N) + 2 * T(pd.N));
         t[2] += 2 * T(pd.M) * C(pd.N);

@@ -1,0 +1,87 @@
+// bpmax_r0only.cuh -- the R0-only double max-plus microbenchmark on the fill's own product
+// kernels. It restates the reference's IPDPSW R0-only program
+// (IPDPSW/source/R0/ospsq_coarse_diag_top_down/ospsq_float.ab:1-15, kernel
+// IPDPSW/source/R0/ospsq_coarse_diag_top_down/src/ospsqmax_float.c:113-189):
+//   F(i1,i1,i2,j2) = seq2[i2]
+//   F(i1,j1,i2,i2) = seq1[i1]                                                  (j1 > i1)
+//   F(i1,j1,i2,j2) = max_{i1<=k1<j1, i2<=k2<j2} F(i1,k1,i2,k2) + F(k1+1,j1,k2+1,j2)   (j1 > i1, j2 > i2)
+// The product kernels evaluate R0 + R3 + R4 as one shifted product whose extra terms read S1 on the
+// subdiagonal of every table (and, for wide tables, the S1 array): with -inf there, they evaluate
+// R0 alone. The finalize of this mode only writes the base values and -inf where the full fill
+// writes S1; the sequences are non-negative, so every value is >= +0 and the product's integer
+// max merge stays exact.
+#pragma once
+#include "bpmax_kernels_large.cuh"
+
+namespace bpmax {
+
+// S1 := -inf for every pair (read by the wide product kernel at row 0 of A and the guard row of B)
+__global__ void r0only_prep_kernel(const PairDesc *__restrict__ pairs, float *__restrict__ S)
+{
+    const PairDesc pd = pairs[blockIdx.x];
+    float *S1 = S + pd.S1_off;
+    for (int q = threadIdx.x; q < pd.M * pd.M; q += blockDim.x) S1[q] = NEG_INF;
+}
+
+// Cell images (Np <= 64), one CTA per outer cell of diagonal d. vals = seq1 (M floats) then seq2
+// (N floats) of the pair, unreversed.
+template <int NP>
+__global__ void __launch_bounds__(128) r0only_finalize_small_kernel(const CellJob *__restrict__ jobs,
+                                                                   const PairDesc *__restrict__ pairs,
+                                                                   float *__restrict__ F,
+                                                                   const float *__restrict__ vals, int d)
+{
+    constexpr int NB = NP / 8, NBLK = NB * (NB + 1) / 2;
+    constexpr long long CELL = 4LL * R0_TAB_COLBASE[NB][NB];
+    const CellJob job = jobs[blockIdx.x];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, i1 = job.i1;
+    float *Fc = F + pd.F_off + cell_index(M, i1, i1 + d) * CELL;
+    const float *v1 = vals, *v2 = vals + M;
+    for (int q4 = threadIdx.x; q4 < NBLK * 16; q4 += blockDim.x) {
+        int BI, BJ;
+        blk_decode(NB, q4 >> 4, BI, BJ);
+        const int r = 8 * BI + ((q4 & 15) >> 1), c0 = 8 * BJ + 4 * (q4 & 1);
+        const int o = 4 * c_img_colbase[NB][BJ] + 68 * BI + 4 * (q4 & 15);  // block (BI, BJ), row r & 7, half
+        const float4 acc = *reinterpret_cast<const float4 *>(Fc + o);
+        const float a[4] = {acc.x, acc.y, acc.z, acc.w};
+        float v[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int c = c0 + t;
+            v[t] = !(r <= c && c < N) ? NEG_INF : (d == 0 ? v2[r] : (r == c ? v1[i1] : a[t]));
+        }
+        *reinterpret_cast<float4 *>(Fc + o) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    if (threadIdx.x < 2 * NB) {  // S1 piece of every block column: all -inf here
+        const int BJ = threadIdx.x >> 1, h = threadIdx.x & 1;
+        *reinterpret_cast<float4 *>(Fc + 4 * c_img_colbase[NB][BJ] + 68 * (BJ + 1) + 4 * h) =
+            make_float4(NEG_INF, NEG_INF, NEG_INF, NEG_INF);
+    }
+}
+
+// Row-major tables and their transposes (Np > 64), one CTA per outer cell of diagonal d.
+__global__ void __launch_bounds__(512) r0only_finalize_wide_kernel(const CellJob *__restrict__ jobs,
+                                                                  const PairDesc *__restrict__ pairs,
+                                                                  float *__restrict__ F, float *__restrict__ FT,
+                                                                  const float *__restrict__ vals, int d)
+{
+    const CellJob job = jobs[blockIdx.x];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1;
+    const long long tile = (long long)Np * Np;
+    float *Fc = F + pd.F_off + cell_index(M, i1, i1 + d) * tile;
+    float *FTc = FT + pd.F_off + cell_index(M, i1, i1 + d) * tile;
+    const float *v1 = vals, *v2 = vals + M;
+    // an off-diagonal value keeps its accumulated maximum, so the transposed read of an entry
+    // another thread rewrites sees the same value either way
+    for (long long q = threadIdx.x; q < tile; q += blockDim.x) {
+        const int r = (int)(q / Np), c = (int)(q % Np);
+        const float f = !(r <= c && c < N) ? NEG_INF : (d == 0 ? v2[r] : (r == c ? v1[i1] : Fc[q]));
+        const float t = !(c <= r && r < N) ? NEG_INF : (d == 0 ? v2[c] : (r == c ? v1[i1] : Fc[(long long)c * Np + r]));
+        Fc[q] = f;
+        FTc[q] = t;
+    }
+}
+
+}  // namespace bpmax

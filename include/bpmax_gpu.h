@@ -67,6 +67,18 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
 int bpmax_gpu_fill_compact(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N,
                            float *F_compact, float *score);
 
+/* R0-only double max-plus microbenchmark on the fill's own product kernels. Replaces the
+ * reference's IPDPSW R0-only program ospsqmax_float(M, N, seq1, seq2, FTable)
+ * (IPDPSW/source/R0/ospsq_coarse_diag_top_down/src/ospsqmax_float.c:113, spec ospsq_float.ab:1-15):
+ *   F(i1,i1,i2,j2) = seq2[i2];  F(i1,j1,i2,i2) = seq1[i1] (j1 > i1);
+ *   F(i1,j1,i2,j2) = max_{i1<=k1<j1, i2<=k2<j2} F(i1,k1,i2,k2) + F(k1+1,j1,k2+1,j2)  (j1 > i1, j2 > i2)
+ * seq1[M], seq2[N]: non-negative integers (converted to float; negative values return EINVAL);
+ * M >= 2, N >= 2 as the reference requires. F_compact (may be NULL) receives the compact layout of
+ * bpmax_gpu_fill_compact (-FLT_MAX where i2 > j2); score (may be NULL) receives F(0,M-1,0,N-1), the
+ * value the reference's program prints. Timing: bpmax_gpu_last_timing. */
+int bpmax_gpu_r0_only(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *F_compact,
+                      float *score);
+
 /* Optimal score F(0,M-1,0,N-1) of one pair, the value V3/bpmax-wrapper.c:281 prints. */
 int bpmax_gpu_score(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, long N, float *score);
 
@@ -117,7 +129,8 @@ int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches);
 /* Re-runs the last fill's kernels one launch at a time with CUDA events around each launch on
  * the context's stream. Per kernel kind k (0 single-strand, 1 R0+R3+R4 product, 2 finalize /
  * inner wavefront): ms[k] = summed launch durations, launches[k] = launch count, terms[k] =
- * algorithmic max-plus candidates (one fp32 add + one max each) the kind evaluates. Arrays of 3.
+ * algorithmic max-plus candidates (one fp32 add + one max each) the kind evaluates (after
+ * bpmax_gpu_r0_only: C(M)C(N) for kind 1, 0 for the others). Arrays of 3.
  * No reference counterpart (measurement only). */
 int bpmax_gpu_profile_kernels(bpmax_ctx *ctx, float *ms, long *launches, double *terms);
 
