@@ -42,6 +42,9 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched pairs/s sub-measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pair", default=None, help="M,N: one custom uniform pair instead of the workload")
+    ap.add_argument("--r0-only", default=None, metavar="M,N",
+                    help="R0-only double max-plus microbenchmark of shape M x N (the reference's IPDPSW program), "
+                         "one JSON line, then exit")
     return ap.parse_args()
 
 
@@ -422,8 +425,71 @@ def measure_batched(eng):
             "autotuned": tuned, "autotune_best_ms": tune_ms}
 
 
+R0_ONLY_PUBLISHED = "246.2 ... 343.8 GFLOPS at 16x1024 ... 16x3000 on a Xeon E-2278G, 8 cores (the reference's own R0-only code)"
+
+
+def r0only_reference_time(M: int, N: int):
+    """The reference's R0-only program (oracle/_ref/ospsqmax_time, random sequences as its driver
+    draws them) on this host's cores: (seconds, threads), or None where it was not built."""
+    from oracle import oracle as O
+
+    if not os.path.exists(O._REF_R0_TIME):
+        return None
+    out = subprocess.run([O._REF_R0_TIME, str(M), str(N)], capture_output=True, text=True, check=True)
+    t = float(next(l for l in out.stdout.splitlines() if l.startswith("Execution time")).split(":")[1].split()[0])
+    return t, os.cpu_count()
+
+
+def main_r0only(args, rank):
+    """R0-only microbenchmark: terms = C(M) C(N) per fill; value = terms / summed device time."""
+    from bpmax_b200 import Engine
+
+    if rank != 0:
+        return
+    M, N = (int(x) for x in args.r0_only.split(","))
+    rng = np.random.default_rng(11)
+    s1 = rng.integers(0, 2**31 - 1, M).astype(np.int32)  # rand()-sized values, as the reference's driver
+    s2 = rng.integers(0, 2**31 - 1, N).astype(np.int32)
+    C = lambda n: n * (n * n - 1) // 6  # noqa: E731
+    terms = C(M) * C(N)
+    eng = Engine(0)
+    peak = eng.maxplus_peak()
+    for _ in range(max(args.warmup, 1)):
+        eng.r0_only(s1, s2, want_table=False)
+    ms = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            eng.r0_only(s1, s2, want_table=False)
+            ms.append(eng.last_timing()[0])
+    prof = eng.profile_kernels()
+    t = sum(ms) / len(ms) * 1e-3
+    v = terms / t / 1e9
+    ms_ = M  # the reference's program on a bounded sample: same N, the largest M' <= M with C(M')C(N) <= 2e11
+    while ms_ > 2 and C(ms_) * C(N) > 2e11:
+        ms_ -= 1
+    sample = (ms_, N)
+    ref = None if args.no_cpu_baseline else r0only_reference_time(*sample)
+    cpu = None
+    if ref:
+        cpu = {"value": C(sample[0]) * C(sample[1]) / ref[0] / 1e9, "unit": "Gterms/s", "cores": ref[1],
+               "kind": "reference", "sample": f"ospsqmax_float {sample[0]}x{sample[1]}, {ref[0]:.3f} s",
+               "host_cpu": host_cpu()}
+    line = {"metric": "R0-only max-plus Gterms/s", "value": v, "unit": "Gterms/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (rand()-sized non-negative integers)",
+            "config": {"workload": f"r0only_{M}x{N}", "M": M, "N": N, "terms_per_step": terms},
+            "gflops": 2 * v, "pct_maxplus_peak": 100.0 * v * 1e9 / peak, "maxplus_peak_Gterms_s": peak / 1e9,
+            "kernels": {k: {"ms": prof[k][0], "launches": prof[k][1]} for k in ("strand", "r0", "finalize")},
+            "published_reference": R0_ONLY_PUBLISHED, "cpu_baseline": cpu, "clocks": clk.summary()}
+    print(json.dumps(line))
+    eng.close()
+
+
 def main():
     args = parse_args()
+    if args.r0_only:
+        main_r0only(args, int(os.environ.get("RANK", "0")))
+        return
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":

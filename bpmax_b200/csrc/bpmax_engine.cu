@@ -339,7 +339,8 @@ void launch_r0only_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     const float *vals = (const float *)ctx->r0vals.p;
     switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
     case 0:
-        r0only_finalize_wide_kernel<<<L.count, 512, 0, s>>>(jobs, pd, (float *)ctx->F.p, (float *)ctx->FT.p, vals, L.d);
+        r0only_finalize_wide_kernel<<<dim3(L.count, L.np / R0ONLY_TILE), 256, 0, s>>>(jobs, pd, (float *)ctx->F.p,
+                                                                                     (float *)ctx->FT.p, vals, L.d);
         break;
     case 1: r0only_finalize_small_kernel<8><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
     case 2: r0only_finalize_small_kernel<16><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;

@@ -60,27 +60,40 @@ __global__ void __launch_bounds__(128) r0only_finalize_small_kernel(const CellJo
     }
 }
 
-// Row-major tables and their transposes (Np > 64), one CTA per outer cell of diagonal d.
-__global__ void __launch_bounds__(512) r0only_finalize_wide_kernel(const CellJob *__restrict__ jobs,
+// Row-major tables and their transposes (Np > 64): CTA (blockIdx.x, blockIdx.y) writes the 32-row
+// band blockIdx.y of cell blockIdx.x of diagonal d, one 32 x 32 tile at a time, and the matching
+// column band of the transpose through a shared tile (coalesced reads and writes on both sides).
+constexpr int R0ONLY_TILE = 32;
+__global__ void __launch_bounds__(256) r0only_finalize_wide_kernel(const CellJob *__restrict__ jobs,
                                                                   const PairDesc *__restrict__ pairs,
                                                                   float *__restrict__ F, float *__restrict__ FT,
                                                                   const float *__restrict__ vals, int d)
 {
+    constexpr int TL = R0ONLY_TILE;
+    __shared__ float tile[TL][TL + 1];
     const CellJob job = jobs[blockIdx.x];
     const PairDesc pd = pairs[job.pair];
     const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1;
-    const long long tile = (long long)Np * Np;
-    float *Fc = F + pd.F_off + cell_index(M, i1, i1 + d) * tile;
-    float *FTc = FT + pd.F_off + cell_index(M, i1, i1 + d) * tile;
+    const long long cell = cell_index(M, i1, i1 + d) * ((long long)Np * Np);
+    float *Fc = F + pd.F_off + cell;
+    float *FTc = FT + pd.F_off + cell;
     const float *v1 = vals, *v2 = vals + M;
-    // an off-diagonal value keeps its accumulated maximum, so the transposed read of an entry
-    // another thread rewrites sees the same value either way
-    for (long long q = threadIdx.x; q < tile; q += blockDim.x) {
-        const int r = (int)(q / Np), c = (int)(q % Np);
-        const float f = !(r <= c && c < N) ? NEG_INF : (d == 0 ? v2[r] : (r == c ? v1[i1] : Fc[q]));
-        const float t = !(c <= r && r < N) ? NEG_INF : (d == 0 ? v2[c] : (r == c ? v1[i1] : Fc[(long long)c * Np + r]));
-        Fc[q] = f;
-        FTc[q] = t;
+    const int tx = threadIdx.x & (TL - 1), ty = threadIdx.x / TL;  // 32 x 8 threads
+    const int r0 = TL * blockIdx.y;
+    for (int c0 = 0; c0 < Np; c0 += TL) {
+#pragma unroll
+        for (int y = ty; y < TL; y += 8) {
+            const int r = r0 + y, c = c0 + tx;
+            const long long q = (long long)r * Np + c;
+            const float f = !(r <= c && c < N) ? NEG_INF : (d == 0 ? v2[r] : (r == c ? v1[i1] : Fc[q]));
+            Fc[q] = f;
+            tile[y][tx] = f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int y = ty; y < TL; y += 8)  // FT[c0 + y][r0 + tx] = F[r0 + tx][c0 + y]
+            FTc[(long long)(c0 + y) * Np + r0 + tx] = tile[tx][y];
+        __syncthreads();
     }
 }
 
