@@ -73,7 +73,9 @@ struct Plan {
     int bases_bytes = 0;
     int maxM = 0;
     // per diagonal and Np class (index NB-1): ranges in the job arrays
-    struct Launch { int d, np, first, count, s1_first = 0, s1_count = 0; };  // np = inner table width class
+    // np = inner table width class; part (product launches): 0 = reads only diagonals <= d-2,
+    // 1 = reads diagonal d-1 too
+    struct Launch { int d, np, first, count, s1_first = 0, s1_count = 0, part = 1; };
     std::vector<Launch> r0_launches, fin_launches;
     std::vector<R0Job> r0_jobs;
     std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > 64 (first/count index this array)
@@ -81,6 +83,7 @@ struct Plan {
     std::vector<int> classes;  // distinct inner widths, ascending
     int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
     bool r0_only = false;  // R0-only double max-plus (bpmax_gpu_r0_only) instead of the BPMax fill
+    bool split = true;     // the product's offset pair 0 may run as its own launch (one-class plans)
     std::vector<cudaEvent_t> diag_ev;  // one pair only: outer diagonal d finalized (recorded by the graph)
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
@@ -95,12 +98,19 @@ struct bpmax_ctx {
     cudaStream_t class_stream[8] = {};  // MAX_CLASS_STREAMS
     cudaStream_t aux_stream = nullptr;  // reference-layout conversion and copy-out, overlapped with the fill
     cudaEvent_t fork_ev = nullptr, join_ev[8] = {};
+    // per width-class chain: a side stream for the product part that reads only diagonals <= d-2,
+    // its completion event, and the chain's finalize events of the last two diagonals
+    cudaStream_t side_stream[8] = {};
+    cudaEvent_t side_done_ev[8] = {}, fin_ev[8][2] = {}, side_join_ev[8] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
     std::string err;
     DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
     DevBuf r0vals;         // R0-only mode: seq1 then seq2 of the pair, as floats
     bool r0_only = false;  // mode of the next prepare()
+    // schedule of the next prepare(): with the reference-layout copy-out running beside the fill
+    // (bpmax_gpu_fill), the unsplit product leaves the SMs the row conversions need
+    bool allow_split = true;
     int r0_occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class NB
     // schedule tunables (bpmax_gpu_set_tuning / bpmax_gpu_autotune); a plan is built with the
     // values current at build time, or with the values an autotune run stored for its shapes
@@ -175,6 +185,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     P.pairs_per_job = ctx->r0_pairs_per_job;
     P.merge_items = ctx->r0_merge_items;
     P.class_streams = ctx->class_streams;
+    P.split = ctx->allow_split;
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
     if (tu != ctx->tuned.end()) {
         P.pairs_per_job = tu->second[0];
@@ -241,9 +252,23 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 const long long P2 = (d + 1) / 2;  // offset pairs per cell
                 const long long resident = (long long)std::max(1, ctx->r0_occ[NB]) * ctx->sms;
                 const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(P.pairs_per_job, qmin);
-                const long long q = r0_pairs_per_job(cells, P2, resident, qmin, qmax, P.merge_items);
+                // Offset pair 0 (offsets 0 and d-1) is the only one that reads diagonal d-1. In a plan
+                // of one width class, where one iteration holds at most 2 items, it becomes its own
+                // launch (part 1) and the other pairs (part 0, reading diagonals <= d-2) can run while
+                // diagonal d-1 is finalized (several classes already overlap each other's finalize).
+                const long long first_pair = (P.split && classes.size() == 1 && G <= 2 && P2 > 1) ? 1 : 0;
+                if (first_pair) {
+                    Plan::Launch rb{d, np, (int)P.r0_jobs.size(), 0};
+                    for (int p = 0; p < n; ++p)
+                        if (P.pairs[p].Np == np && Ms[p] > d)
+                            for (int i1 = 0; i1 < Ms[p] - d; ++i1) P.r0_jobs.push_back(R0Job{p, i1, 0, 1});
+                    rb.count = (int)P.r0_jobs.size() - rb.first;
+                    P.r0_launches.push_back(rb);
+                }
+                const long long q = r0_pairs_per_job(cells, P2 - first_pair, resident, qmin, qmax, P.merge_items);
                 Plan::Launch rl{d, np, (int)P.r0_jobs.size(), 0};
-                for (long long c0 = 0; c0 < P2; c0 += q)
+                rl.part = first_pair ? 0 : 1;
+                for (long long c0 = first_pair; c0 < P2; c0 += q)
                     for (int p = 0; p < n; ++p)
                         if (P.pairs[p].Np == np && Ms[p] > d)
                             for (int i1 = 0; i1 < Ms[p] - d; ++i1)
@@ -420,58 +445,89 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
     // pairs of different inner widths never interact: each width class runs its own chain of
     // diagonals on its own stream (parallel branches of the captured graph); profiling runs
     // serialise everything on the main stream so every launch can be timed
-    const bool fork = !(kp && kp->on) && P.classes.size() > 1 && P.class_streams;
-    auto stream_of = [&](int np) {
-        if (!fork) return ctx->stream;
-        const int k = (int)(std::find(P.classes.begin(), P.classes.end(), np) - P.classes.begin());
-        return ctx->class_stream[k % MAX_CLASS_STREAMS];
+    const bool prof = kp && kp->on;
+    const bool fork = !prof && P.classes.size() > 1 && P.class_streams;
+    auto chain_of = [&](int np) {
+        if (!fork) return 0;
+        return (int)(std::find(P.classes.begin(), P.classes.end(), np) - P.classes.begin()) % MAX_CLASS_STREAMS;
     };
+    auto stream_of = [&](int np) { return fork ? ctx->class_stream[chain_of(np)] : ctx->stream; };
     const int nstreams = fork ? std::min((int)P.classes.size(), MAX_CLASS_STREAMS) : 0;
-    if (fork) {
+    // product launches that read only diagonals <= d-2 (part 0) run on each chain's side stream,
+    // after the finalize of d-2, so they overlap the finalize of d-1; the chain's finalize of d
+    // waits for them
+    bool any_part0 = false;
+    for (const auto &L : P.r0_launches) any_part0 = any_part0 || L.part == 0;
+    const bool split = !prof && any_part0;
+    const int nside = split ? std::max(nstreams, 1) : 0;
+    if (fork || split) {
         CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
         for (int k = 0; k < nstreams; ++k) CK(cudaStreamWaitEvent(ctx->class_stream[k], ctx->fork_ev, 0));
+        for (int k = 0; k < nside; ++k) CK(cudaStreamWaitEvent(ctx->side_stream[k], ctx->fork_ev, 0));
     }
+    bool side_pending[MAX_CLASS_STREAMS] = {};
     size_t ri = 0, fi = 0;
     for (int d = 0; d < P.maxM; ++d) {
         for (; ri < P.r0_launches.size() && P.r0_launches[ri].d == d; ++ri, ++launches) {
             const auto &L = P.r0_launches[ri];
-            const cudaStream_t st = stream_of(L.np);
-            ProfScope ps(ctx, kp, 1);
-            switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-            case 0: launch_r0_large(ctx, L, st); break;
-            case 1: launch_r0<1>(ctx, L, st); break;
-            case 2: launch_r0<2>(ctx, L, st); break;
-            case 3: launch_r0<3>(ctx, L, st); break;
-            case 4: launch_r0<4>(ctx, L, st); break;
-            case 5: launch_r0<5>(ctx, L, st); break;
-            case 6: launch_r0<6>(ctx, L, st); break;
-            case 7: launch_r0<7>(ctx, L, st); break;
-            default: launch_r0<8>(ctx, L, st); break;
+            const int c = chain_of(L.np);
+            cudaStream_t st = stream_of(L.np);
+            if (split && L.part == 0) {
+                st = ctx->side_stream[c];
+                if (d >= 2) CK(cudaStreamWaitEvent(st, ctx->fin_ev[c][d & 1], 0));  // finalize of d-2
+            }
+            {
+                ProfScope ps(ctx, kp, 1);
+                switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
+                case 0: launch_r0_large(ctx, L, st); break;
+                case 1: launch_r0<1>(ctx, L, st); break;
+                case 2: launch_r0<2>(ctx, L, st); break;
+                case 3: launch_r0<3>(ctx, L, st); break;
+                case 4: launch_r0<4>(ctx, L, st); break;
+                case 5: launch_r0<5>(ctx, L, st); break;
+                case 6: launch_r0<6>(ctx, L, st); break;
+                case 7: launch_r0<7>(ctx, L, st); break;
+                default: launch_r0<8>(ctx, L, st); break;
+                }
+            }
+            if (split && L.part == 0) {
+                CK(cudaEventRecord(ctx->side_done_ev[c], st));
+                side_pending[c] = true;
             }
         }
         for (; fi < P.fin_launches.size() && P.fin_launches[fi].d == d; ++fi, ++launches) {
             const auto &L = P.fin_launches[fi];
+            const int c = chain_of(L.np);
             const cudaStream_t st = stream_of(L.np);
-            ProfScope ps(ctx, kp, 2);
-            if (P.r0_only) {
-                launch_r0only_fin(ctx, L, st);
-                continue;
+            if (side_pending[c]) CK(cudaStreamWaitEvent(st, ctx->side_done_ev[c], 0));
+            {
+                ProfScope ps(ctx, kp, 2);
+                if (P.r0_only) {
+                    launch_r0only_fin(ctx, L, st);
+                } else {
+                    switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
+                    case 0: launch_fin_large(ctx, L, st); break;
+                    case 1: launch_fin<1>(ctx, L, st); break;
+                    case 2: launch_fin<2>(ctx, L, st); break;
+                    case 3: launch_fin<3>(ctx, L, st); break;
+                    case 4: launch_fin<4>(ctx, L, st); break;
+                    case 5: launch_fin<5>(ctx, L, st); break;
+                    case 6: launch_fin<6>(ctx, L, st); break;
+                    case 7: launch_fin<7>(ctx, L, st); break;
+                    default: launch_fin<8>(ctx, L, st); break;
+                    }
+                }
             }
-            switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-            case 0: launch_fin_large(ctx, L, st); break;
-            case 1: launch_fin<1>(ctx, L, st); break;
-            case 2: launch_fin<2>(ctx, L, st); break;
-            case 3: launch_fin<3>(ctx, L, st); break;
-            case 4: launch_fin<4>(ctx, L, st); break;
-            case 5: launch_fin<5>(ctx, L, st); break;
-            case 6: launch_fin<6>(ctx, L, st); break;
-            case 7: launch_fin<7>(ctx, L, st); break;
-            default: launch_fin<8>(ctx, L, st); break;
-            }
+            if (split) CK(cudaEventRecord(ctx->fin_ev[c][d & 1], st));
         }
+        for (bool &p : side_pending) p = false;
         // outer diagonal d is final: rows of the reference layout that end on it can be copied out
-        if (!P.diag_ev.empty() && !(kp && kp->on))
+        if (!P.diag_ev.empty() && !prof)
             CK(cudaEventRecordWithFlags(P.diag_ev[d], ctx->stream, cudaEventRecordExternal));
+    }
+    for (int k = 0; k < nside; ++k) {  // join the side streams back into the main stream
+        CK(cudaEventRecord(ctx->side_join_ev[k], ctx->side_stream[k]));
+        CK(cudaStreamWaitEvent(ctx->stream, ctx->side_join_ev[k], 0));
     }
     for (int k = 0; k < nstreams; ++k) {  // join the class chains back into the main stream
         CK(cudaEventRecord(ctx->join_ev[k], ctx->class_stream[k]));
@@ -494,7 +550,8 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
                                         : std::array<int, 3>{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams};
     const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
                              ctx->plan.class_streams == want[2];
-    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only)) {
+    if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only &&
+          ctx->plan.split == ctx->allow_split)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
         ctx->plan.graph = nullptr;
         for (cudaEvent_t e : ctx->plan.diag_ev) cudaEventDestroy(e);
@@ -700,7 +757,12 @@ int bpmax_gpu_create(int device, bpmax_ctx **out)
     if (st == BPMAX_OK && cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking) != cudaSuccess) st = BPMAX_ECUDA;
     for (int k = 0; k < MAX_CLASS_STREAMS && st == BPMAX_OK; ++k)
         if (cudaStreamCreateWithFlags(&ctx->class_stream[k], cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&ctx->side_stream[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->side_done_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->side_join_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->fin_ev[k][0], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ctx->fin_ev[k][1], cudaEventDisableTiming) != cudaSuccess)
             st = BPMAX_ECUDA;
     if (st == BPMAX_OK) st = set_smem_attr<1>(ctx);
     if (st == BPMAX_OK) st = set_smem_attr<2>(ctx);
@@ -726,7 +788,8 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
     for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs,
-                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs, &ctx->scores, &ctx->conv, &ctx->errflag})
+                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs, &ctx->scores, &ctx->conv, &ctx->errflag,
+                      &ctx->r0vals})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
         if (ctx->host_stage[i]) cudaFreeHost(ctx->host_stage[i]);
@@ -740,6 +803,9 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     for (int k = 0; k < MAX_CLASS_STREAMS; ++k) {
         if (ctx->class_stream[k]) cudaStreamDestroy(ctx->class_stream[k]);
         if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
+        if (ctx->side_stream[k]) cudaStreamDestroy(ctx->side_stream[k]);
+        for (cudaEvent_t e : {ctx->side_done_ev[k], ctx->side_join_ev[k], ctx->fin_ev[k][0], ctx->fin_ev[k][1]})
+            if (e) cudaEventDestroy(e);
     }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -869,7 +935,10 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
     if ((st = ensure(ctx, ctx->conv, 2 * row_max * sizeof(float))) != BPMAX_OK) return st;
     const bool pinned = is_pinned(F_lin);
     if (!pinned && (st = ensure_host_stage(ctx, row_max * sizeof(float))) != BPMAX_OK) return st;
-    if ((st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N, true)) != BPMAX_OK) return st;
+    ctx->allow_split = false;
+    st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N, true);
+    ctx->allow_split = true;
+    if (st != BPMAX_OK) return st;
     const std::vector<cudaEvent_t> &dev = ctx->plan.diag_ev;
     std::vector<long long> pending_n(2, 0);
     std::vector<float *> pending_dst(2, nullptr);
