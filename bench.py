@@ -8,7 +8,12 @@ One step = one complete fill of one sequence pair (default: strand 1 N1=1024, st
 uniform random ACGU from a seed, integer weights GC=3/AU=2/GU=1). One term = one max-plus
 candidate (one fp32 add + one max); a fill evaluates C(M)C(N) + 2T(M)C(N) + 2C(M)T(N) + C(M) + C(N)
 terms with C(n) = n(n^2-1)/6, T(n) = n(n+1)/2 (twice this is the reference's "bpmax OPS").
-With N GPUs every rank fills its own pair (independent pairs, no collective): weak scaling.
+With N GPUs every rank fills its own pair (independent pairs, no collective): weak scaling; a batched
+workload is split over the ranks by estimated work instead (strong scaling), its scores gathered once.
+The default line also carries the sub-measurements of the other configurations (batched pairs/s,
+the balanced 256 x 256 pair, the forward + adjoint batch), bitwise windows of the benched tables
+against the reference's own fill ("parity"), and the reference's fill of a bounded sample timed on
+the host cores ("cpu_baseline").
 Prints ONE JSON line on rank 0.
 """
 from __future__ import annotations
@@ -19,6 +24,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -69,8 +75,8 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="bpmax_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         q = "clocks.sm,clocks.max.sm,power.draw," + ",".join("clocks_event_reasons." + c for c in REASON_COLS)
@@ -156,40 +162,98 @@ def reduce_max(world, x: float, device: str = "cuda") -> float:
 
 
 # ---------------------------------------------------------------------------------- CPU side
-def cpu_sample_pair(wl_name: str):
-    """Bounded sample of the workload for the reference's CPU fill: same strand-2 length and
-    weights, strand 1 shortened so one fill takes ~10-20 s on 16 host cores."""
-    if wl_name in ("single", "grad"):
-        return W.single_pair(160, 64, seed=2), 32, "strand1 N1=160 prefix-size pair, strand2 N2=64, N_tile=32 (3x8)"
-    if wl_name == "small":
-        return W.single_pair(128, 32, seed=1), 16, "the full pair N1=128, N2=32, N_tile=16 (3x8)"
-    if wl_name == "balanced":
-        return W.single_pair(24, 256, seed=3), 64, "strand1 N1=24, strand2 N2=256, N_tile=64 (3x8)"
-    return W.single_pair(100, 40, seed=4), 8, "one pair N1=100, N2=40, N_tile=8 (3x8)"
+# Windows of the benched pairs that the reference fills on the host cores: F(i1, j1, ., .) with
+# j1 < K depends only on seq1[0..K) and seq2, and with i1 >= M-K only on seq1[M-K..M), so the
+# reference's fill of the prefix pair (seq1[:K], seq2) holds exactly the cells j1 < K of the full
+# table and the fill of the suffix pair the cells i1 >= M-K. The prefix fill is also the bounded
+# CPU sample that is timed (about 10 s of work on 16 host cores).
+SAMPLES = {  # workload -> (prefix K, suffix K, N_tile of the reference fill)
+    "single": (160, 96, 32),
+    "small": (128, 0, 16),
+    "balanced": (24, 24, 64),
+    "grad": (160, 0, 32),
+}
+
+
+def cpu_sample(wl_name: str, wl: W.Workload):
+    """(prefix pair workload, N_tile, description) of the bounded CPU sample of ``wl``."""
+    if wl_name == "batched":  # the batch's first pair with N2 >= 9 (the reference needs N_sec >= 2, NR = 8)
+        a, b = next(p for p in wl.pairs if len(p[1]) >= 9)
+        n = len(b)
+        T = 8 if n <= 16 else (16 if n <= 32 else 32)
+        return W.Workload(f"batched_pair_{len(a)}x{n}", [(a, b)], wl.weights), T, \
+            f"one pair of the batch, N1={len(a)}, N2={n}, N_tile={T} (3x8)"
+    K, _, T = SAMPLES[wl_name]
+    a, b = wl.pairs[0]
+    K = min(K, len(a))
+    what = "the full pair" if K == len(a) else f"the strand-1 prefix seq1[:{K}] of the benched pair"
+    return W.Workload(f"{wl.name}_prefix{K}", [(a[:K], b)], wl.weights), T, \
+        f"{what}, N1={K}, N2={len(b)}, N_tile={T} (3x8)"
 
 
 def run_reference_fill(pair_wl: W.Workload, n_tile: int):
+    """The reference's own fill (oracle/_ref, all host cores) of one pair, timed around its bpmax()
+    call alone as V3/bpmax-wrapper.c:274-284 times it. Returns (terms, seconds, threads, table)."""
     from oracle import oracle as O
 
     s1, s2 = pair_wl.pairs[0]
     threads = min(os.cpu_count() or 1, 128)
-    t0 = time.perf_counter()
-    out = O.ref_fill(s1, s2, pair_wl.weights, n_tile, 3, 8, threads=threads, sentinel=0.0)
-    dt = time.perf_counter() - t0
+    out, dt = O.ref_fill(s1, s2, pair_wl.weights, n_tile, 3, 8, threads=threads, sentinel=0.0, timed=True)
     terms = W.terms(len(s1), len(s2))["total"]
     return terms, dt, threads, out
 
 
-def cpu_baseline(wl_name: str):
+def cpu_baseline(wl_name: str, wl: W.Workload):
+    """Returns (cpu_baseline dict, (reference table of the prefix pair, K, N_tile) or None)."""
     from oracle import oracle as O
 
     if not O.ref_available():
         return {"value": None, "unit": "Gterms/s", "cores": None, "kind": "reference",
-                "sample": "oracle/_ref not built (needs the reference sources at build time)"}
-    wl, T, desc = cpu_sample_pair(wl_name)
-    terms, dt, threads, _ = run_reference_fill(wl, T)
-    return {"value": terms / dt / 1e9, "unit": "Gterms/s", "cores": threads, "kind": "reference",
-            "sample": f"{desc}; {terms:.3e} terms in {dt:.2f} s", "host_cpu": host_cpu()}
+                "sample": "oracle/_ref not built (needs the reference sources at build time)"}, None
+    swl, T, desc = cpu_sample(wl_name, wl)
+    terms, dt, threads, out = run_reference_fill(swl, T)
+    return ({"value": terms / dt / 1e9, "unit": "Gterms/s", "cores": threads, "kind": "reference",
+             "sample": f"{desc}; {terms:.3e} terms in {dt:.2f} s (bpmax() alone)", "host_cpu": host_cpu()},
+            (out, len(swl.pairs[0][0]), T))
+
+
+def windows_vs_reference(eng, wl: W.Workload, K_pre: int, K_suf: int, T: int, ref_pre=None):
+    """Bitwise comparison of windows of the engine's last fill (the full-size pair of ``wl``) with
+    the reference's own fills of the prefix and suffix pairs: every cell the reference writes for
+    the outer cells j1 < K_pre, and i1 >= M - K_suf. ref_pre: the prefix table when already filled."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return {"checked": False, "why": "oracle/_ref not built"}
+    s1, s2 = wl.pairs[0]
+    M, N = len(s1), len(s2)
+    out = {"against": "the reference's own fill (oracle/_ref) of the prefix / suffix pair, bitwise on every "
+                      "cell it writes (reference layout, masks and halo rows included)", "N_tile": T}
+    total_cells = total_bad = 0
+    for name, K, lo in (("prefix", K_pre, 0), ("suffix", K_suf, M - K_suf)):
+        if K <= 0:
+            continue
+        K = min(K, M)
+        lo = 0 if name == "prefix" else M - K
+        sub = s1[:K] if name == "prefix" else s1[M - K:]
+        if name == "prefix" and ref_pre is not None and ref_pre[1] == K and ref_pre[2] == T:
+            ref = ref_pre[0]
+        else:
+            ref = O.ref_fill(sub, s2, wl.weights, T, 3, 8, sentinel=0.0)
+        win = eng.read_cells(0, lo, lo + K, lo, lo + K, N)
+        iu, ju = np.triu_indices(K)
+        mine = O.to_reference_layout(np.ascontiguousarray(win[iu, ju]), K, N, T)
+        mask = O.reference_written_mask(K, N, T)
+        bad = int(np.count_nonzero(mine.view(np.uint32)[mask] != ref.view(np.uint32)[mask]))
+        cells = int(np.count_nonzero(mask))
+        out[name] = {"outer_cells": f"{'j1' if name == 'prefix' else 'i1'} {'<' if name == 'prefix' else '>='} "
+                                    f"{K if name == 'prefix' else M - K}", "K": K, "cells": cells, "mismatches": bad}
+        total_cells += cells
+        total_bad += bad
+        del win, mine, mask, ref
+    out["cells"] = total_cells
+    out["mismatches"] = total_bad
+    return out
 
 
 def host_cpu() -> str:
@@ -218,12 +282,13 @@ def mem_available_bytes() -> int:
 def main_reference(args, world, rank):
     if rank != 0:
         return
-    wl, T, desc = cpu_sample_pair(args.workload)
     from oracle import oracle as O
 
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbpmax_ref.so was not built"}))
         return
+    full = workload(args.workload, 0, args.pair)
+    wl, T, desc = cpu_sample(args.workload, full)
     for _ in range(args.warmup):
         run_reference_fill(wl, T)
     tot_terms, tot_t = 0, 0.0
@@ -235,9 +300,10 @@ def main_reference(args, world, rank):
     line = {"metric": "max-plus Gterms/s", "value": v, "unit": "Gterms/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl.name, "sample_of": args.workload, "N_tile": T, "MR": 3, "NR": 8},
+            "config": {"workload": full.name, "sample_pair": wl.name, "N_tile": T, "MR": 3, "NR": 8},
             "cpu_baseline": {"value": v, "unit": "Gterms/s", "cores": threads, "kind": "reference",
-                             "sample": desc, "host_cpu": host_cpu()},
+                             "sample": f"{desc}; each step one fill of it, timed around bpmax() alone",
+                             "host_cpu": host_cpu()},
             "e2e": {"value": v, "unit": "Gterms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -246,25 +312,33 @@ def main_reference(args, world, rank):
 def main_b200(args, world, rank, local):
     from bpmax_b200 import Engine
 
-    wl = workload(args.workload, rank, args.pair)
+    single = args.workload in ("single", "small", "balanced") or bool(args.pair)
+    # one pair: every rank fills its own (weak scaling); a batch: the same batch on every rank, each
+    # filling its LPT share by estimated work (strong scaling), scores gathered at the end
+    wl = workload(args.workload, rank if single else 0, args.pair)
     eng = Engine(local)
     eng.set_weights(wl.weights)
-    single = len(wl.pairs) == 1
     terms_step = wl.total_terms
     s1, s2 = wl.pairs[0]
+    mine = list(range(len(wl.pairs)))
+    if not single and world > 1:
+        from bpmax_b200 import shard
+
+        mine = shard.shares_of(wl.pairs, world)[rank]
+    my_pairs = [wl.pairs[i] for i in mine]
 
     def step():
         if single:
             eng.score(s1, s2)
         elif args.workload == "grad":
-            eng.grad_batch(wl.pairs)
+            eng.grad_batch(my_pairs)
         else:
-            eng.score_batch(wl.pairs)
+            eng.score_batch(my_pairs)
         return eng.last_timing()
 
     tuned = None
     if not single:  # batches: schedule chosen by the autotuner on these shapes (outside the timing)
-        tuned, _ = eng.autotune(wl.pairs, trials=1)
+        tuned, _ = eng.autotune(my_pairs, trials=1)
     for _ in range(max(args.warmup, 0)):
         step()
     barrier(world)
@@ -279,7 +353,13 @@ def main_b200(args, world, rank, local):
         wall = time.perf_counter() - t0
     clocks = clk.summary()
     dev_ms = reduce_max(world, dev_ms)
-    value = terms_step * args.steps * world / (dev_ms * 1e-3) / 1e9
+    value = terms_step * args.steps * (world if single else 1) / (dev_ms * 1e-3) / 1e9
+    gathered = None
+    if not single and world > 1:  # every rank's scores into batch order (one object all-gather)
+        from bpmax_b200 import shard
+
+        scores, _ = shard.run_sharded(eng.score_batch, wl.pairs, rank, world)
+        gathered = {"pairs": int(len(scores)), "ranks": world, "my_pairs": len(mine)}
 
     # roofline: eager re-run with events around every launch
     prof = eng.profile_kernels()
@@ -289,43 +369,56 @@ def main_b200(args, world, rank, local):
     roofline["kernels"] = {k: {"ms": v[0], "launches": v[1], "terms": v[2]} for k, v in prof.items()}
     roofline["r0_share_of_step"] = r0_ms / sum(v[0] for v in prof.values())
 
-    e2e = None
-    if not args.no_e2e and single and len(s2) >= 8:
-        e2e = measure_e2e(eng, wl, args, world)
-
-    batched = None
-    if not args.no_batched and single and args.workload == "single" and not args.pair and world == 1:
-        batched = measure_batched(eng)
-        eng.set_weights(wl.weights)
-
-    cpu = None
+    # the reference's own fill of a bounded sample (the prefix pair), and bitwise windows of the
+    # benched table against the reference (rank 0 of a one-GPU run; the engine still holds the table)
+    cpu, parity, ref_pre = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(args.workload)
+            cpu, ref_pre = cpu_baseline(args.workload, wl)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)}
+        if single and args.workload in SAMPLES:
+            K_pre, K_suf, T = SAMPLES[args.workload]
+            try:
+                parity = windows_vs_reference(eng, wl, K_pre, K_suf, T, ref_pre)
+            except Exception as e:
+                parity = {"checked": False, "error": str(e)}
+
+    e2e = None
+    if not args.no_e2e and single and len(s2) >= 8:
+        e2e = measure_e2e(eng, wl, args, world, ref_pre)
+
+    extra = {}
+    if not args.no_batched and single and args.workload == "single" and not args.pair and world == 1:
+        extra["batched"] = measure_batched(eng)
+        extra["balanced"] = measure_balanced(eng, peak, with_reference=not args.no_cpu_baseline)
+        extra["grad"] = measure_grad(eng)
+        eng.set_weights(wl.weights)
 
     if rank == 0:
         M, N = len(s1), len(s2)
         line = {"metric": "max-plus Gterms/s", "value": value, "unit": "Gterms/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "impl": "b200",
+                "higher_is_better": True, "scaling": "weak" if single else "strong", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "impl": "b200",
                 "config": {"workload": wl.name, "N1": M if single else None, "N2": N if single else None,
                            "pairs": len(wl.pairs), "terms_per_step": terms_step,
                            "weights": [float(x) for x in wl.weights],
                            "l2": "inputs larger than L2 (each step streams its F tables from HBM)",
-                           "parallelism": f"independent pairs per rank x{world}", "autotuned": tuned},
+                           "parallelism": (f"independent pairs per rank x{world}" if single else
+                                           f"batch sharded over {world} ranks by estimated work (LPT)"),
+                           "autotuned": tuned, "gathered": gathered},
                 "pct_maxplus_peak": 100.0 * value * 1e9 / peak,
                 "gpu_launches": launches, "wall_s": wall, "clocks": clocks, "roofline": roofline,
-                "cpu_baseline": cpu, "e2e": e2e, "batched": batched}
+                "cpu_baseline": cpu, "parity": parity, "e2e": e2e, **extra}
         print(json.dumps(line))
     eng.close()
 
 
 # DRAM bytes (read + write) per product item (one outer cell and one k1) of the R0 kernel with
-# inner width 64, from one ncu capture of a 512x64 fill (profiles/r0_kernel_512x64.md): the
-# kernel's traffic grows with the items it processes.
+# inner width 64: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of a 512 x 64 fill
+# (outer diagonal 256: 256 cells x 256 items, 1.079 GB) divided by its items. The kernel's traffic
+# grows with the items it processes, so a launch's traffic is this figure times its items.
 R0_DRAM_BYTES_PER_ITEM_NP64 = 16466
 
 
@@ -357,7 +450,7 @@ def r0_roofline(wl, r0_ms, r0_n, r0_terms, peak_terms_s, clocks):
         hbm = measured_peaks().get("hbm_gbs")
         source = "MEASURED_PEAKS.json hbm_gbs (of measured)"
         if not hbm:
-            hbm, source = 6650.0, "6.65 TB/s copy bandwidth measured earlier on this pool (of fallback)"
+            hbm, source = 6650.0, "6.65 TB/s, an earlier copy-bandwidth measurement on a B200 (of fallback)"
         gbs = traffic / per_launch_s / 1e9
         out["hbm"] = {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
                       "peak_source": source,
@@ -373,9 +466,11 @@ def measured_peaks() -> dict:
         return {}
 
 
-def measure_e2e(eng, wl, args, world):
+def measure_e2e(eng, wl, args, world, ref_pre=None):
     """The same fill through the reference-facing C call bpmax_gpu_fill: sequences from host
-    memory in, the whole F table in the reference's layout back into pinned host memory."""
+    memory in, the whole F table in the reference's layout back into pinned host memory. With the
+    reference's own fill of the prefix pair (ref_pre = (table, K, N_tile)), the last step's table is
+    also compared with it, bitwise on every cell the reference writes for the outer cells j1 < K."""
     s1, s2 = wl.pairs[0]
     M, N = len(s1), len(s2)
     T = 32 if N >= 64 else (16 if N >= 32 else 8)
@@ -395,10 +490,23 @@ def measure_e2e(eng, wl, args, world):
         _, score = eng.fill(s1, s2, T, out=out)
     barrier(world)
     wall = reduce_max(world, time.perf_counter() - t0)
+    res = {"value": wl.total_terms * args.steps * world / wall / 1e9, "unit": "Gterms/s",
+           "h2d_bytes_per_step": 4 * (M + N), "d2h_bytes_per_step": d2h, "N_tile": T,
+           "api": "bpmax_gpu_fill (reference layout, pinned host buffer)", "s_per_step": wall / args.steps}
+    if ref_pre is not None and ref_pre[2] == T:
+        from oracle import oracle as O
+
+        ref, K, _ = ref_pre
+        cell_f = ns * ns * (T + 1) * T
+        mine = np.ascontiguousarray(out.reshape(M, M, cell_f)[:K, :K])
+        mask = O.reference_written_mask(K, N, T)
+        bad = int(np.count_nonzero(mine.reshape(-1).view(np.uint32)[mask] != ref.view(np.uint32)[mask]))
+        res["parity_reference_layout"] = {"outer_cells": f"j1 < {K}", "cells": int(np.count_nonzero(mask)),
+                                          "mismatches": bad,
+                                          "against": "the reference's own fill of the prefix pair (oracle/_ref)"}
+        del mine, mask
     del out, buf
-    return {"value": wl.total_terms * args.steps * world / wall / 1e9, "unit": "Gterms/s",
-            "h2d_bytes_per_step": 4 * (M + N), "d2h_bytes_per_step": d2h, "N_tile": T,
-            "api": "bpmax_gpu_fill (reference layout, pinned host buffer)", "s_per_step": wall / args.steps}
+    return res
 
 
 def measure_batched(eng):
@@ -423,6 +531,54 @@ def measure_batched(eng):
             "speedup": ms_e / mb, "terms": wl.total_terms, "Gterms_per_s_batched": wl.total_terms / (mb * 1e-3) / 1e9,
             "launches_per_pair_launch": launches_e, "wall_s_per_pair_pass": wall_e / 2,
             "autotuned": tuned, "autotune_best_ms": tune_ms}
+
+
+def measure_balanced(eng, peak, with_reference=True):
+    """Configuration 3: one 256 x 256 pair, uniform and GC-rich (P(G) = P(C) = 0.35): fill rate, the
+    product kernel's roofline, and bitwise windows against the reference's own fill."""
+    out = {}
+    for tag, gc in (("uniform", False), ("gc_rich", True)):
+        wl = W.single_pair(256, 256, seed=3, gc_rich=gc)
+        s1, s2 = wl.pairs[0]
+        eng.set_weights(wl.weights)
+        eng.score(s1, s2)  # warm-up (captures the graph)
+        ms = []
+        for _ in range(2):
+            eng.score(s1, s2)
+            ms.append(eng.last_timing()[0])
+        t = statistics.median(ms)
+        d = {"workload": wl.name, "ms_per_fill": t, "value": wl.total_terms / (t * 1e-3) / 1e9, "unit": "Gterms/s"}
+        if not gc:
+            prof = eng.profile_kernels()
+            r0_ms, r0_n, r0_terms = prof["r0"]
+            d["roofline"] = r0_roofline(wl, r0_ms, r0_n, r0_terms, peak, {})
+            d["roofline"]["kernels"] = {k: {"ms": v[0], "launches": v[1], "terms": v[2]} for k, v in prof.items()}
+        if with_reference:
+            K_pre, K_suf, T = SAMPLES["balanced"]
+            try:
+                d["parity"] = windows_vs_reference(eng, wl, K_pre, K_suf, T)
+            except Exception as e:
+                d["parity"] = {"checked": False, "error": str(e)}
+        out[tag] = d
+    return out
+
+
+def measure_grad(eng):
+    """Configuration 5: 64 pairs of 256 x 64, 12 weights from U[0.5, 4]: the forward fill plus the
+    adjoint pass (exact d score / d weights); pairs/s with the forward / backward split."""
+    wl = W.gradient_batch(64, 256, 64, seed=5)
+    eng.set_weights(wl.weights)
+    eng.grad_batch(wl.pairs)  # warm-up (captures the graph)
+    fwd, tot = [], []
+    for _ in range(2):
+        eng.score_batch(wl.pairs)
+        fwd.append(eng.last_timing()[0])
+        eng.grad_batch(wl.pairs)
+        tot.append(eng.last_timing()[0])
+    f, t = statistics.median(fwd), statistics.median(tot)
+    return {"workload": wl.name, "pairs": len(wl.pairs), "pairs_per_s": len(wl.pairs) / (t * 1e-3),
+            "ms_forward": f, "ms_backward": t - f, "ms_total": t,
+            "Gterms_per_s_forward": wl.total_terms / (f * 1e-3) / 1e9}
 
 
 R0_ONLY_PUBLISHED = "246.2 ... 343.8 GFLOPS at 16x1024 ... 16x3000 on a Xeon E-2278G, 8 cores (the reference's own R0-only code)"

@@ -66,6 +66,8 @@ def load_library():
     L.bpmax_gpu_profile_kernels.argtypes = [vp, vp, vp, vp]
     L.bpmax_gpu_maxplus_peak.argtypes = [vp, P(ctypes.c_double)]
     L.bpmax_gpu_score_noalloc.argtypes = [vp, c_long, vp, c_long, vp, vp, vp]
+    L.bpmax_gpu_read_cells.argtypes = [vp, c_int, c_long, c_long, c_long, c_long, vp]
+    L.bpmax_gpu_shim_set_weights.argtypes = [vp]
     L.bpmax_gpu_set_tuning.argtypes = [vp, c_int, c_long]
     L.bpmax_gpu_get_tuning.argtypes = [vp, c_int, P(c_long)]
     L.bpmax_gpu_autotune.argtypes = [vp, c_int, vp, vp, vp, vp, c_int, vp, P(c_float)]
@@ -208,7 +210,17 @@ class Engine:
         self._check(self._L.bpmax_gpu_grad_batch(self._ctx, n, p1, _ptr(Ms), p2, _ptr(Ns), _ptr(scores), _ptr(grads)))
         return scores, grads
 
-    TUNING_KEYS = {"r0_pairs_per_job": 0, "r0_merge_items": 1, "class_streams": 2}
+    def read_cells(self, pair: int, i1_lo: int, i1_hi: int, j1_lo: int, j1_hi: int, N: int) -> np.ndarray:
+        """bpmax_gpu_read_cells: inner tables of outer cells [i1_lo, i1_hi) x [j1_lo, j1_hi) of pair
+        ``pair`` of the last fill, as float32 [i1, j1, N, N] (-FLT_MAX where i2 > j2, NaN where
+        i1 > j1). N is that pair's strand-2 length."""
+        out = np.empty((i1_hi - i1_lo, j1_hi - j1_lo, N, N), dtype=np.float32)
+        self._check(self._L.bpmax_gpu_read_cells(self._ctx, int(pair), int(i1_lo), int(i1_hi), int(j1_lo), int(j1_hi),
+                                                 _ptr(out)))
+        return out
+
+    TUNING_KEYS = {"r0_pairs_per_job": 0, "r0_merge_items": 1, "class_streams": 2, "wait_limit_us": 3,
+                   "inject_wait_timeout": 4}
 
     def set_tuning(self, key: str, value: int) -> None:
         self._check(self._L.bpmax_gpu_set_tuning(self._ctx, self.TUNING_KEYS[key], int(value)))

@@ -117,6 +117,10 @@ struct bpmax_ctx {
     int r0_pairs_per_job = 1 << 20;                 // upper bound of k1 offset pairs per product job
     int r0_merge_items = 2;                         // cost of one job merge, in items, for job sizing
     int class_streams = 1;                          // run the width classes of a batch on parallel streams
+    // bounded waits of the product kernels: time limit of one wait, and the one-shot test mode in
+    // which the next fill's product kernels issue no copies (their first waits run out)
+    unsigned long long wait_ns = 4000000000ULL;
+    bool inject_wait_timeout = false;
     std::map<std::vector<int>, std::array<int, 3>> tuned;  // shape signature (Ms then Ns) -> tunables
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
@@ -158,6 +162,11 @@ int ensure(bpmax_ctx *ctx, DevBuf &b, size_t bytes)
     CK(cudaMalloc(&b.p, want));
     b.bytes = want;
     return BPMAX_OK;
+}
+
+WaitCtl wait_ctl(const bpmax_ctx *ctx)
+{
+    return WaitCtl{(int *)ctx->errflag.p, ctx->wait_ns, ctx->inject_wait_timeout ? 1 : 0};
 }
 
 int weights_ok(const float *w)
@@ -335,7 +344,7 @@ void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     const int grid = std::min(L.count, std::max(1, ctx->r0_occ[NB]) * ctx->sms);  // resident CTAs; each loops over jobs
     r0_kernel<NB><<<grid, C::THREADS, C::SMEM, s>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
                                                               (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
-                                                              (int *)ctx->errflag.p);
+                                                              wait_ctl(ctx));
 }
 
 template <int NB, int T>
@@ -446,6 +455,9 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
     // diagonals on its own stream (parallel branches of the captured graph); profiling runs
     // serialise everything on the main stream so every launch can be timed
     const bool prof = kp && kp->on;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(ctx->stream, &cap));
+    const bool capturing = cap == cudaStreamCaptureStatusActive;
     const bool fork = !prof && P.classes.size() > 1 && P.class_streams;
     auto chain_of = [&](int np) {
         if (!fork) return 0;
@@ -473,6 +485,17 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
             const int c = chain_of(L.np);
             cudaStream_t st = stream_of(L.np);
             if (split && L.part == 0) {
+                // Part 0 of diagonal d (offset pairs >= 1) may run beside the finalize of d-1 because:
+                //  1. it reads only tables of diagonals <= d-2, and waits here for the finalize of d-2,
+                //     the last writer of those tables and of the SW1 candidates pushed into the still
+                //     cleared tables of diagonal d (a finalize of diagonal e writes only the tables of
+                //     e, the S1 pieces of e and the pushes into e+2);
+                //  2. it writes the tables of diagonal d only through atomicMax of partial maxima,
+                //     which commutes with part 1's merges and with those pushes (all values >= +0);
+                //  3. the finalize of d-1 writes no table of diagonal d, and the finalize of d waits
+                //     for both parts (side_done_ev below).
+                // A finalize that wrote diagonal d, or a product merge that was not an atomic max,
+                // would race here.
                 st = ctx->side_stream[c];
                 if (d >= 2) CK(cudaStreamWaitEvent(st, ctx->fin_ev[c][d & 1], 0));  // finalize of d-2
             }
@@ -522,7 +545,8 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         }
         for (bool &p : side_pending) p = false;
         // outer diagonal d is final: rows of the reference layout that end on it can be copied out
-        if (!P.diag_ev.empty() && !prof)
+        // (events recorded as external nodes of the captured graph; eager runs record none)
+        if (!P.diag_ev.empty() && !prof && capturing)
             CK(cudaEventRecordWithFlags(P.diag_ev[d], ctx->stream, cudaEventRecordExternal));
     }
     for (int k = 0; k < nside; ++k) {  // join the side streams back into the main stream
@@ -611,6 +635,16 @@ int launch_fill(bpmax_ctx *ctx)
 {
     Plan &P = ctx->plan;
     int st;
+    if (ctx->inject_wait_timeout) {  // test of the timeout path: one eager run, outside the graph
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        if ((st = enqueue_fill(ctx, P)) != BPMAX_OK) return st;
+        for (cudaEvent_t e : P.diag_ev) CK(cudaEventRecord(e, ctx->stream));  // copy-out waits for the whole fill
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        gather_scores_kernel<<<((int)P.pairs.size() + 127) / 128, 128, 0, ctx->stream>>>(
+            (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)P.pairs.size(), (float *)ctx->scores.p);
+        CK(cudaGetLastError());
+        return BPMAX_OK;
+    }
     if (!P.graph) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -645,7 +679,11 @@ int finish_fill(bpmax_ctx *ctx)
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
     ctx->last_launches = P.launches + 1;  // + the score gather
-    if (errv) return fail(ctx, BPMAX_ETIMEOUT, "a product kernel gave up waiting for its operand copies");
+    const bool injected = ctx->inject_wait_timeout;
+    ctx->inject_wait_timeout = false;  // one-shot
+    if (errv)
+        return fail(ctx, BPMAX_ETIMEOUT, "a product kernel gave up waiting for its operand copies%s",
+                    injected ? " (test mode: no copies were issued)" : "");
     return BPMAX_OK;
 }
 
@@ -1082,6 +1120,17 @@ int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value)
     case BPMAX_TUNE_CLASS_STREAMS:
         ctx->class_streams = value != 0;
         break;
+    case BPMAX_TUNE_WAIT_LIMIT_US:
+        if (value < 1 || value > 600000000L) return fail(ctx, BPMAX_EINVAL, "wait limit out of range (1 us .. 600 s)");
+        ctx->wait_ns = (unsigned long long)value * 1000ULL;
+        if (ctx->plan.graph) {  // a kernel argument baked into the captured graph: recapture on next use
+            cudaGraphExecDestroy(ctx->plan.graph);
+            ctx->plan.graph = nullptr;
+        }
+        break;
+    case BPMAX_TUNE_INJECT_WAIT_TIMEOUT:
+        ctx->inject_wait_timeout = value != 0;
+        break;
     default: return fail(ctx, BPMAX_EINVAL, "unknown tuning key %d", key);
     }
     return BPMAX_OK;
@@ -1094,6 +1143,8 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value)
     case BPMAX_TUNE_R0_PAIRS_PER_JOB: *value = ctx->r0_pairs_per_job; break;
     case BPMAX_TUNE_R0_MERGE_ITEMS: *value = ctx->r0_merge_items; break;
     case BPMAX_TUNE_CLASS_STREAMS: *value = ctx->class_streams; break;
+    case BPMAX_TUNE_WAIT_LIMIT_US: *value = (long)(ctx->wait_ns / 1000ULL); break;
+    case BPMAX_TUNE_INJECT_WAIT_TIMEOUT: *value = ctx->inject_wait_timeout ? 1 : 0; break;
     default: return BPMAX_EINVAL;
     }
     return BPMAX_OK;
@@ -1148,6 +1199,29 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
     return BPMAX_OK;
 }
 
+int bpmax_gpu_read_cells(bpmax_ctx *ctx, int pair, long i1_lo, long i1_hi, long j1_lo, long j1_hi, float *out)
+{
+    if (!ctx) return BPMAX_EINVAL;
+    if (!ctx->plan_valid) return fail(ctx, BPMAX_EINVAL, "no fill has run on this context");
+    const Plan &P = ctx->plan;
+    if (pair < 0 || pair >= (int)P.pairs.size()) return fail(ctx, BPMAX_EINVAL, "pair %d out of range", pair);
+    const PairDesc &pd = P.pairs[pair];
+    if (!out || i1_lo < 0 || j1_lo < 0 || i1_lo >= i1_hi || j1_lo >= j1_hi || i1_hi > pd.M || j1_hi > pd.M)
+        return fail(ctx, BPMAX_EINVAL, "outer cell window [%ld,%ld) x [%ld,%ld) outside 0..%d", i1_lo, i1_hi, j1_lo,
+                    j1_hi, pd.M);
+    CK(cudaSetDevice(ctx->device));
+    const long long n_out = (long long)(i1_hi - i1_lo) * (j1_hi - j1_lo) * pd.N * pd.N;
+    int st;
+    if ((st = ensure(ctx, ctx->conv, n_out * sizeof(float))) != BPMAX_OK) return st;
+    read_cells_kernel<<<4 * ctx->sms, 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p + pair, (const float *)ctx->F.p,
+                                                             (int)i1_lo, (int)j1_lo, (int)(j1_hi - j1_lo), n_out,
+                                                             (float *)ctx->conv.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, ctx->conv.p, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return BPMAX_OK;
+}
+
 int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches)
 {
     if (!ctx) return BPMAX_EINVAL;
@@ -1172,6 +1246,7 @@ int bpmax_gpu_last_timing(const bpmax_ctx *ctx, float *fill_ms, long *launches)
 namespace {
 
 constexpr size_t NOALLOC_FLOATS = (size_t)16 << 20;  // 64 MiB of fp32 scratch
+constexpr unsigned long long NOALLOC_WAIT_NS = 4000000000ULL;  // time limit of one bounded wait
 
 static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_FLOATS];
 
@@ -1254,7 +1329,7 @@ void noalloc_launch_diag(cudaStream_t s, const NoallocDevice &nd, int d, int n_r
 {
     if (d > 0)
         r0_kernel<NB><<<std::min(n_r0, std::max(1, nd.occ[NB]) * nd.sms), R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM, s>>>(
-            rj, n_r0, pd, F, d, err);
+            rj, n_r0, pd, F, d, WaitCtl{err, NOALLOC_WAIT_NS, 0});
     const int n_s1 = n_cells - 1;  // S1 cells of diagonal d+1: the first n_cells-1 entries of cj
     using Sh = FinShape<8 * NB>;
     finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
@@ -1273,6 +1348,8 @@ extern "C" int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2,
     for (long i = 0; i < N; ++i)
         if (seq2[i] < 0 || seq2[i] > 4) return BPMAX_EINVAL;
     if (!weights_ok(weights12)) return BPMAX_EINVAL;
+    // an error left pending by the caller's own earlier work is not this call's to report or clear
+    if (cudaPeekAtLastError() != cudaSuccess) return BPMAX_ECUDA;
     const int Np = std::max(8, (int)(N + 7) / 8 * 8);
     const int nb = Np / 8;
     // scratch layout (floats), every region 256-byte aligned

@@ -387,6 +387,24 @@ __global__ void to_compact_kernel(const PairDesc *__restrict__ pdp, const float 
     }
 }
 
+// inner tables of the outer cells (i1, j1), i1 in [i1_lo, i1_lo+nI), j1 in [j1_lo, j1_lo+nJ), of one
+// pair -> out[i1-i1_lo][j1-j1_lo][N][N]; -FLT_MAX where i2 > j2, NaN for outer cells with i1 > j1
+__global__ void read_cells_kernel(const PairDesc *__restrict__ pdp, const float *__restrict__ F, int i1_lo, int j1_lo,
+                                  int nJ, long long n_out, float *__restrict__ out)
+{
+    const PairDesc pd = *pdp;
+    const long long NN = (long long)pd.N * pd.N;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n_out;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long oc = q / NN;
+        const int i1 = i1_lo + (int)(oc / nJ), j1 = j1_lo + (int)(oc % nJ);
+        const int r = (int)((q % NN) / pd.N), c = (int)(q % pd.N);
+        float v = __int_as_float(0x7fc00000);
+        if (i1 <= j1) v = r <= c ? f_value(pd, F, cell_index(pd.M, i1, j1), r, c) : -3.402823466e+38f;
+        out[q] = v;
+    }
+}
+
 __global__ void gather_scores_kernel(const PairDesc *__restrict__ pairs, const float *__restrict__ F, int num_pairs,
                                      float *__restrict__ scores)
 {

@@ -88,7 +88,8 @@ struct R0Cfg {
     static constexpr int OFF_DST = OFF_RED + 4 * RED_WORDS;
     static constexpr int OFF_BAR = (OFF_DST + 4 * NBLK + 15) / 16 * 16;
     static constexpr int OFF_CNT = OFF_BAR + 8 * STAGES;  // per stage: warps done with it
-    static constexpr size_t SMEM = (size_t)OFF_CNT + 4 * STAGES;
+    static constexpr int OFF_ARM = OFF_CNT + 4 * STAGES;  // per stage: phases armed (expect_tx) so far
+    static constexpr size_t SMEM = (size_t)OFF_ARM + 4 * STAGES;
     static constexpr int WARPS = THREADS / 32;
     // warp program of each warp, 2 bits per warp (0 full task, 1 diagonal A, 2 diagonal B, 3 both)
     static constexpr unsigned ROLE_BITS = R0_TAB_ROLE[NB][0] | R0_TAB_ROLE[NB][1] << 2 | R0_TAB_ROLE[NB][2] << 4 |
@@ -108,19 +109,42 @@ __device__ __forceinline__ void mbar_arrive_tx(unsigned bar, unsigned bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// bounded wait for the completion of phase `parity` of an mbarrier; false when the bound ran out
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+// Control of the bounded waits of the product kernels (kernel argument, one per launch).
+//   err:      device word set to 1 when a wait gives up (read by the host: BPMAX_ETIMEOUT)
+//   wait_ns:  how long one wait may poll, in %globaltimer nanoseconds
+//   inject:   1 = issue no operand copies at all, so the first wait of every CTA runs out with no
+//             copy in flight (the host's test of the timeout path); 0 in every ordinary fill
+struct WaitCtl {
+    int *err;
+    unsigned long long wait_ns;
+    int inject;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
 {
-    for (int tries = 0; tries < (1 << 24); ++tries) {
-        unsigned ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the completion of phase `parity` of an mbarrier: polls until the phase
+// completes or limit_ns have passed since the first unsuccessful poll; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try(bar, parity))
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    return true;
 }
 // global -> shared bulk copy on the TMA engine (16-byte aligned addresses, size a multiple of 16)
 __device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar)
@@ -188,7 +212,7 @@ __device__ __forceinline__ void r0_task(const float *__restrict__ As, const floa
 template <int NB>
 __global__ void __launch_bounds__(R0Cfg<NB>::THREADS, R0Cfg<NB>::MINB)
 r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs, float *__restrict__ F, int d,
-          int *__restrict__ err)
+          WaitCtl ctl)
 {
     using C = R0Cfg<NB>;
     constexpr int S = C::STAGES;
@@ -200,6 +224,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
                                                                                           // block in a cell image
     uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(smem) + C::OFF_BAR);
     int *done_cnt = reinterpret_cast<int *>(reinterpret_cast<char *>(smem) + C::OFF_CNT);
+    int *armed = reinterpret_cast<int *>(reinterpret_cast<char *>(smem) + C::OFF_ARM);  // phases armed per stage
     const int tid = threadIdx.x;
     int jid = blockIdx.x;
     if (jid >= njobs) return;
@@ -208,6 +233,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
         for (int s = 0; s < S; ++s) {
             mbar_init(smem_u32(bars + s), 1);
             done_cnt[s] = 0;
+            armed[s] = 0;
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -237,10 +263,11 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
     const unsigned smem_base = smem_u32(smem);
     const int lane = tid & 31;
     // announces the bytes of iteration `it` of a job of `items` items on stage s's mbarrier (one
-    // thread, before any copy of that iteration is issued)
+    // thread, before any copy of that iteration is issued), and counts the stage's armed phases
     auto expect = [&](int s, int items, int it) {
         const int valid = min(C::G, items - it * C::G);
         mbar_arrive_tx(smem_u32(bars + s), (unsigned)(valid * C::ITEM_TX));
+        armed[s] += 1;
     };
     // issues the copies (whole cell images) of iteration `it` of job j into stage s, spread over
     // the threads me, me+count, ... (the job record is re-read here: positions are kept as indices,
@@ -272,7 +299,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
             if (j_ < njobs) items_ = r0_job_items(jobs[j_], d);
         }
     };
-    if (tid == 0) {  // expected bytes of the first S iterations (every stage starts free)
+    if (tid == 0 && !ctl.inject) {  // expected bytes of the first S iterations (every stage starts free)
         int j_ = pj, it_ = pit, items_ = pitems;
         for (int s = 0; s < S && j_ < njobs; ++s) {
             expect(s, items_, it_);
@@ -283,7 +310,7 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
 #pragma unroll 1
     for (int s = 0; s < S; ++s)
         if (pj < njobs) {
-            issue(s, pj, pit, tid, C::THREADS);
+            if (!ctl.inject) issue(s, pj, pit, tid, C::THREADS);
             advance(pj, pitems, pit);
         }
 
@@ -295,12 +322,16 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
 
     unsigned phase = 0;  // bit s: parity of stage s's next completion
     int stage = 0;
-    bool bad = false;    // an mbarrier wait ran out: skip waits and work, leave at the next job end
+    // bad: a wait of this thread ran out. It then skips waits and work, arms and issues no more
+    // copies, and the CTA leaves at the next job end after waiting (bounded) for the copies it
+    // already issued, so none is left in flight into the shared memory of a finished CTA. This path
+    // is best-effort: if those copies do not land within the limit either, the CTA leaves anyway.
+    bool bad = false;
 #pragma unroll 1
     while (true) {
         const bool active = has_task && it * C::G + tg < items;
-        if (!bad && !mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u)) {
-            atomicExch(err, 1);
+        if (!bad && !mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u, ctl.wait_ns)) {
+            atomicExch(ctl.err, 1);
             bad = true;
         }
         phase ^= 1u << stage;
@@ -324,12 +355,13 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
                 for (int j = 0; j < 8; ++j) acc[0][j] = fmaxf(acc[0][j], s1a + rv[j]);
             }
         }
-        // the last warp done with this stage refills it with the iteration S ahead
+        // the last warp done with this stage refills it with the iteration S ahead (not after a
+        // timeout: the other warps' waits on the unarmed phase then run out too)
         __syncwarp();
         int last = 0;
         if (lane == 0) last = atomicAdd(done_cnt + stage, 1) == C::WARPS - 1;
         last = __shfl_sync(0xffffffffu, last, 0);
-        if (last && pj < njobs) {
+        if (last && pj < njobs && !__any_sync(0xffffffffu, bad) && !ctl.inject) {
             if (lane == 0) {
                 done_cnt[stage] = 0;
                 expect(stage, pitems, pit);
@@ -354,7 +386,12 @@ r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict_
                         acc[i][j] = NEG_INF;
                     }
             }
-            if (__syncthreads_or(bad)) return;
+            if (__syncthreads_or(bad)) {  // no thread arms or issues from here on
+                if (tid == 0)
+                    for (int s = 0; s < S; ++s)
+                        if (armed[s] > 0) mbar_wait(smem_u32(bars + s), (unsigned)(armed[s] - 1) & 1u, ctl.wait_ns);
+                return;
+            }
             int *out = reinterpret_cast<int *>(F + pd.F_off + cell_index(pd.M, job.i1, job.i1 + d) * CELL);
             for (int e = tid; e < 64 * C::NBLK; e += C::THREADS) {
                 const int q = e >> 6, w = e & 63;

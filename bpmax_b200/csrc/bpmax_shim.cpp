@@ -9,6 +9,7 @@
 // CPU register tiles and thread count; the GPU ignores them. R is recomputed from N and N_tile
 // (the wrapper leaves it uninitialised when N % N_tile == 0, V3/bpmax-wrapper.c:158-167).
 // Weights are the reference's hard-coded ones unless bpmax_gpu_shim_set_weights() changed them.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -31,9 +32,12 @@ float g_w[12] = {1.0f, 1.0f, 3.0f, 3.0f, 1.5f, 1.5f, 1.0f, 1.0f, 3.0f, 3.0f, 1.5
 
 extern "C" int bpmax_gpu_shim_set_weights(const float *w12)
 {
+    if (!w12) return BPMAX_EINVAL;
+    for (int t = 0; t < 12; ++t)
+        if (!std::isfinite(w12[t]) || w12[t] < 0.0f || std::signbit(w12[t])) return BPMAX_EINVAL;
     std::lock_guard<std::mutex> lk(g_mu);
     memcpy(g_w, w12, sizeof g_w);
-    return 0;
+    return BPMAX_OK;
 }
 
 void bpmax(long M, long N, long N_sec, long N_tile, long R, long MR, long NR, long P, int *seq1, int *seq2,

@@ -46,6 +46,14 @@ const char *bpmax_gpu_status_string(int status);
  * Replaces the link-time hook e_intra_score/e_inter_score, V3/external_functions.c:58-68. */
 int bpmax_gpu_set_weights(bpmax_ctx *ctx, const float *weights12);
 
+/* Weights of the drop-in bpmax() symbol this library exports (the reference's C++ entry point,
+ * V3/bpmax.c:129). The reference reads its weights through the link-time hooks
+ * e_intra_score/e_inter_score (V3/external_functions.c:58-68), which a library cannot see; this
+ * sets the weights every later bpmax() call of the process uses (12 entries as above; default:
+ * the reference's hard-coded values). EINVAL for a NULL pointer or a weight that is not finite
+ * and >= +0, leaving the previous weights in place. Thread-safe. */
+int bpmax_gpu_shim_set_weights(const float *weights12);
+
 /* Fill of one pair into the reference's linear F layout, host memory:
  * F_lin = &FTable[0][0][0][0][0][0] of a float[M][M][N_sec][N_sec][N_tile+1][N_tile] buffer,
  * N_sec = ceil(N/N_tile), R = (N_tile - N % N_tile) % N_tile, logical cell
@@ -104,11 +112,20 @@ int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s,
  * compile-time tile sizes and the MR/NR/P arguments of bpmax(), V3/bpmax.c:129).
  *   BPMAX_TUNE_R0_PAIRS_PER_JOB  upper bound of k1 offset pairs (w, d-1-w) per product job (>= 1)
  *   BPMAX_TUNE_R0_MERGE_ITEMS    cost of one job's merge, in items, used to size the jobs of a diagonal
- *   BPMAX_TUNE_CLASS_STREAMS     1: width classes of a batch run as parallel graph branches; 0: one chain */
+ *   BPMAX_TUNE_CLASS_STREAMS     1: width classes of a batch run as parallel graph branches; 0: one chain
+ *   BPMAX_TUNE_WAIT_LIMIT_US     how long one device-side wait of a product kernel for its operand
+ *                                copies may last before the kernel gives up and the call returns
+ *                                BPMAX_ETIMEOUT (microseconds, 1 .. 600e6; default 4e6 = 4 s)
+ *   BPMAX_TUNE_INJECT_WAIT_TIMEOUT  1: the next fill call (only that one) runs its product kernels
+ *                                without issuing any operand copy, so their first waits run out with
+ *                                no copy in flight; the call returns BPMAX_ETIMEOUT and later calls
+ *                                are unaffected. A test of the timeout path; 0 otherwise. */
 enum bpmax_tuning_key {
     BPMAX_TUNE_R0_PAIRS_PER_JOB = 0,
     BPMAX_TUNE_R0_MERGE_ITEMS = 1,
-    BPMAX_TUNE_CLASS_STREAMS = 2
+    BPMAX_TUNE_CLASS_STREAMS = 2,
+    BPMAX_TUNE_WAIT_LIMIT_US = 3,
+    BPMAX_TUNE_INJECT_WAIT_TIMEOUT = 4
 };
 int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value);
 int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value);
@@ -121,6 +138,14 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value);
  * every fill are unchanged by any setting (bit for bit). No reference counterpart. */
 int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
                        const int *const *seq2s, const long *Ns, int trials, long *best, float *best_ms);
+
+/* Copies part of the last fill's table to host memory: the inner tables of the outer cells (i1, j1)
+ * with i1 in [i1_lo, i1_hi) and j1 in [j1_lo, j1_hi) of pair `pair` of that fill (0 for a single
+ * pair), as out[i1 - i1_lo][j1 - j1_lo][N][N] floats, [i2][j2] over the reversed strand 2 as in
+ * bpmax_gpu_fill_compact; -FLT_MAX where i2 > j2 and NaN for outer cells with i1 > j1. Lets a
+ * caller read a window of a table too large to copy whole (no reference counterpart: the
+ * reference's caller owns the whole table in host memory, V3/bpmax-wrapper.c:175-197). */
+int bpmax_gpu_read_cells(bpmax_ctx *ctx, int pair, long i1_lo, long i1_hi, long j1_lo, long j1_hi, float *out);
 
 /* Device time in milliseconds of the last fill call's kernels (CUDA events on the context's
  * stream), and the number of kernel launches it issued. */
@@ -154,7 +179,8 @@ int bpmax_gpu_maxplus_peak(bpmax_ctx *ctx, double *terms_per_s);
  * call on a device looks up the array's device address and sets kernel attributes for that
  * device (make it before any stream capture). Every call reuses the same array, so calls that overlap on the GPU (other threads,
  * other streams) race and must be serialised by the caller. Errors are returned as status codes
- * only (there is no context to hold a message). */
+ * only (there is no context to hold a message); a CUDA error already pending on the calling thread
+ * when the call starts is left in place and reported as BPMAX_ECUDA. */
 int bpmax_gpu_score_noalloc(const int *seq1, long M, const int *seq2, long N, const float *weights12,
                             float *score, void *stream);
 

@@ -35,10 +35,28 @@ _lib = None
 _ref = None
 
 
-def build() -> None:
-    """Compile the checkers (make -C oracle). The reference part only builds where the
-    reference sources exist."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+_REF_CLI = os.path.join(HERE, "_ref", "bpmax_gpu_cli")              # the reference's CLI wrapper on the GPU library
+_REF_CLI_CHECK = os.path.join(HERE, "_ref", "bpmax_gpu_cli_check")  # the same, -DCHECKING -DNO_PROMPT
+
+
+def reference_root() -> str | None:
+    """The reference project's root: $REFERENCE_ROOT, else its mount in the build container."""
+    root = os.environ.get("REFERENCE_ROOT") or "/root/reference"
+    return root if os.path.isdir(root) else None
+
+
+def build(targets=()) -> None:
+    """Compile the checkers (make -C oracle). The parts built from the reference's sources only
+    build where those sources exist."""
+    cmd = ["make", "-s", "-C", HERE]
+    root = reference_root()
+    if root:
+        cmd.append(f"REFERENCE_ROOT={root}")
+    subprocess.run(cmd + list(targets), check=True)
+
+
+def cli_available() -> bool:
+    return os.path.exists(_REF_CLI) and os.path.exists(_REF_CLI_CHECK)
 
 
 def lib():
@@ -75,6 +93,9 @@ def ref():
         L = ctypes.CDLL(_REF)
         L.ref_bpmax_fill.argtypes = [_L, _L, _L, _L, _L, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, ctypes.c_int]
         L.ref_bpmax_fill.restype = ctypes.c_int
+        L.ref_bpmax_fill_timed.argtypes = [_L, _L, _L, _L, _L, ctypes.c_int, _i32p, _i32p, _f32p, _f32p, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)]
+        L.ref_bpmax_fill_timed.restype = ctypes.c_int
         L.ref_bpmax_verify.argtypes = [_L, _L, _i32p, _i32p, _f32p, _f32p]
         L.ref_bpmax_verify.restype = ctypes.c_int
         _ref = L
@@ -206,17 +227,20 @@ def logical_from_reference(F_ref, M: int, N: int, T: int) -> np.ndarray:
 
 
 def ref_fill(seq1, seq2, w12, N_tile: int, MR: int = 3, NR: int = 8, threads: int | None = None,
-             sentinel=np.nan, zero_scratch: bool = True) -> np.ndarray:
-    """Reference fill into its own linear layout; unwritten cells keep ``sentinel``."""
+             sentinel=np.nan, zero_scratch: bool = True, timed: bool = False):
+    """Reference fill into its own linear layout; unwritten cells keep ``sentinel``. With
+    ``timed`` returns (table, seconds of the bpmax() call alone)."""
     s1, s2, w = _as(seq1), _as(seq2), _w(w12)
     M, N = len(s1), len(s2)
     out = np.full(reference_size(M, N, N_tile), sentinel, dtype=np.float32)
     if threads is None:
         threads = min(os.cpu_count() or 1, 128)
-    rc = ref().ref_bpmax_fill(M, N, N_tile, MR, NR, threads, s1, s2, w, out, int(zero_scratch))
+    secs = ctypes.c_double(0.0)
+    rc = ref().ref_bpmax_fill_timed(M, N, N_tile, MR, NR, threads, s1, s2, w, out, int(zero_scratch),
+                                    ctypes.byref(secs))
     if rc != 0:
         raise ValueError("reference fill rejected its arguments")
-    return out
+    return (out, secs.value) if timed else out
 
 
 def ref_verify(seq1, seq2, w12) -> np.ndarray:

@@ -29,6 +29,7 @@
 #include <fcntl.h>
 #include <malloc.h>
 #include <omp.h>
+#include <chrono>
 #include <unistd.h>
 #include <xmmintrin.h>
 
@@ -96,8 +97,11 @@ void ref_set_weights(const float *w12);
 // Fills the caller's reference-layout buffer F_lin
 // (M*M*N_sec*N_sec*(N_tile+1)*N_tile floats). Returns 0, or -1 for parameters the reference
 // rejects with exit(-1) (V3/bpmax.c:131) or that would overrun its register tiles.
-int ref_bpmax_fill(long M, long N, long N_tile, long MR, long NR, int threads, const int *seq1,
-                   const int *seq2, const float *w12, float *F_lin, int zero_scratch)
+// seconds (may be NULL) receives the wall time of the bpmax() call alone, the interval the
+// reference's CLI wrapper times (V3/bpmax-wrapper.c:274-284); the pointer tree, the sequence
+// copies and the FTZ/DAZ switch are outside it.
+int ref_bpmax_fill_timed(long M, long N, long N_tile, long MR, long NR, int threads, const int *seq1,
+                         const int *seq2, const float *w12, float *F_lin, int zero_scratch, double *seconds)
 {
     if (M < 1 || N < 8 || N_tile < 4 || MR < 1 || NR < 1 || threads < 1 || threads > 128) return -1;
     long N_sec = (N + N_tile - 1) / N_tile;
@@ -130,7 +134,10 @@ int ref_bpmax_fill(long M, long N, long N_tile, long MR, long NR, int threads, c
     {
         QuietStdout quiet;
         FtzDaz ftz(threads);
+        const auto t0 = std::chrono::steady_clock::now();
         bpmax(M, N, N_sec, N_tile, R, MR, NR, threads, s1, s2, F);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
     }
     if (zero_scratch) mallopt(M_PERTURB, 0);
     free(s1);
@@ -147,6 +154,12 @@ int ref_bpmax_fill(long M, long N, long N_tile, long MR, long NR, int threads, c
     }
     free(F);
     return 0;
+}
+
+int ref_bpmax_fill(long M, long N, long N_tile, long MR, long NR, int threads, const int *seq1,
+                   const int *seq2, const float *w12, float *F_lin, int zero_scratch)
+{
+    return ref_bpmax_fill_timed(M, N, N_tile, MR, NR, threads, seq1, seq2, w12, F_lin, zero_scratch, nullptr);
 }
 
 // Runs the reference's memoised verify program into F4 (M*M*N*N floats, [i1][j1][i2][j2],

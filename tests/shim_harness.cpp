@@ -1,12 +1,19 @@
 // Drop-in check: a caller written like the reference's CLI wrapper (V3/bpmax-wrapper.c:175-197
 // allocation, :277 call) links against libbpmax_gpu.so and calls the C++ bpmax() symbol.
-// Usage: shim_harness M N N_tile out.bin  (reads M then N base codes from stdin)
+// Usage: shim_harness M N N_tile out.bin [w1 .. w12]  (reads M then N base codes from stdin;
+// with 12 weights, sets them through bpmax_gpu_shim_set_weights before the call)
 #include <cstdio>
 #include <cstdlib>
 void bpmax(long, long, long, long, long, long, long, long, int *, int *, float ******);
+extern "C" int bpmax_gpu_shim_set_weights(const float *w12);
 int main(int argc, char **argv)
 {
     if (argc < 5) return 2;
+    if (argc >= 17) {
+        float w[12];
+        for (int t = 0; t < 12; ++t) w[t] = (float)atof(argv[5 + t]);
+        if (bpmax_gpu_shim_set_weights(w) != 0) return 4;
+    }
     long M = atol(argv[1]), N = atol(argv[2]), T = atol(argv[3]);
     long Ns = (N + T - 1) / T, R = (T - N % T) % T;
     int *s1 = (int *)malloc(sizeof(int) * M), *s2 = (int *)malloc(sizeof(int) * N);
