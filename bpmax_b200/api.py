@@ -220,7 +220,9 @@ class Engine:
         return out
 
     TUNING_KEYS = {"r0_pairs_per_job": 0, "r0_merge_items": 1, "class_streams": 2, "wait_limit_us": 3,
-                   "inject_wait_timeout": 4}
+                   "inject_wait_timeout": 4, "wide_stages": 5, "r0_variant": 6}
+    #: the tunables bpmax_gpu_autotune chooses, in the order it reports them
+    AUTOTUNED = ("r0_pairs_per_job", "r0_merge_items", "class_streams", "r0_variant", "wide_stages")
 
     def set_tuning(self, key: str, value: int) -> None:
         self._check(self._L.bpmax_gpu_set_tuning(self._ctx, self.TUNING_KEYS[key], int(value)))
@@ -234,11 +236,11 @@ class Engine:
         """bpmax_gpu_autotune: times the candidate schedules on these pairs and keeps the fastest
         for their shapes. Returns ({tunable: value}, fill ms)."""
         n, p1, p2, Ms, Ns, keep = self._batch_args(pairs)
-        best = np.zeros(3, dtype=np.int64)
+        best = np.zeros(len(self.AUTOTUNED), dtype=np.int64)
         ms = ctypes.c_float()
         self._check(self._L.bpmax_gpu_autotune(self._ctx, n, p1, _ptr(Ms), p2, _ptr(Ns), int(trials), _ptr(best),
                                                ctypes.byref(ms)))
-        return {k: int(best[i]) for k, i in self.TUNING_KEYS.items()}, float(ms.value)
+        return {k: int(best[i]) for i, k in enumerate(self.AUTOTUNED)}, float(ms.value)
 
     def profile_kernels(self):
         """Per kernel kind (strand, r0, finalize): (ms, launches, terms) of an eager re-run of

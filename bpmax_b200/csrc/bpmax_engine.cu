@@ -28,10 +28,15 @@
 #include "bpmax_r0.cuh"
 #include "bpmax_adjoint.cuh"
 #include "bpmax_r0only.cuh"
+#include "bpmax_wide.cuh"
 
 using namespace bpmax;
 
 namespace {
+
+// schedule tunables in key order: pairs per job, merge cost, class streams, product shape variant,
+// tile-product stages
+using Tuned = std::array<int, 5>;
 
 constexpr int MAX_SMALL_NP = 64;
 constexpr int MAX_CLASS_STREAMS = 8;  // side streams for the per-width-class chains of a batch
@@ -69,7 +74,7 @@ struct Plan {
     std::vector<int> Ms, Ns;
     std::vector<PairDesc> pairs;
     long long F_floats = 0, S_floats = 0;
-    bool any_wide = false;  // some pair has Np > 64 (row-major tables + FT)
+    bool any_large = false;  // some pair has Np > WIDE_TILE_MAX_NP (row-major tables + FT)
     int bases_bytes = 0;
     int maxM = 0;
     // per diagonal and Np class (index NB-1): ranges in the job arrays
@@ -78,10 +83,12 @@ struct Plan {
     struct Launch { int d, np, first, count, s1_first = 0, s1_count = 0, part = 1; };
     std::vector<Launch> r0_launches, fin_launches;
     std::vector<R0Job> r0_jobs;
-    std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > 64 (first/count index this array)
+    std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > WIDE_TILE_MAX_NP (first/count index this array)
+    std::vector<R0JobW> r0w_jobs;  // jobs of launches with tile-image tables (first/count index this array)
     std::vector<CellJob> cell_jobs;
     std::vector<int> classes;  // distinct inner widths, ascending
     int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
+    int r0_variant = 0, wide_stages = 2;
     bool r0_only = false;  // R0-only double max-plus (bpmax_gpu_r0_only) instead of the BPMax fill
     bool split = true;     // the product's offset pair 0 may run as its own launch (one-class plans)
     std::vector<cudaEvent_t> diag_ev;  // one pair only: outer diagonal d finalized (recorded by the graph)
@@ -105,23 +112,26 @@ struct bpmax_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     Weights W;
     std::string err;
-    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
+    DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, r0wjobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
     DevBuf r0vals;         // R0-only mode: seq1 then seq2 of the pair, as floats
     bool r0_only = false;  // mode of the next prepare()
     // schedule of the next prepare(): with the reference-layout copy-out running beside the fill
     // (bpmax_gpu_fill), the unsplit product leaves the SMs the row conversions need
     bool allow_split = true;
-    int r0_occ[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // resident product CTAs per SM, per width class NB
+    int r0_occ_v[2][9] = {};  // resident product CTAs per SM, per shape variant and width class NB
+    int wide_occ[4] = {};     // resident tile-product CTAs per SM, per stage count
     // schedule tunables (bpmax_gpu_set_tuning / bpmax_gpu_autotune); a plan is built with the
     // values current at build time, or with the values an autotune run stored for its shapes
     int r0_pairs_per_job = 1 << 20;                 // upper bound of k1 offset pairs per product job
     int r0_merge_items = 2;                         // cost of one job merge, in items, for job sizing
     int class_streams = 1;                          // run the width classes of a batch on parallel streams
+    int r0_variant = 0;                             // shape variant of the width-64 product kernel (0 or 1)
+    int wide_stages = 2;                            // shared-memory stages of the tile-image product (2 or 3)
     // bounded waits of the product kernels: time limit of one wait, and the one-shot test mode in
     // which the next fill's product kernels issue no copies (their first waits run out)
     unsigned long long wait_ns = 4000000000ULL;
     bool inject_wait_timeout = false;
-    std::map<std::vector<int>, std::array<int, 3>> tuned;  // shape signature (Ms then Ns) -> tunables
+    std::map<std::vector<int>, Tuned> tuned;  // shape signature (Ms then Ns) -> tunables
     float *host_stage[2] = {nullptr, nullptr};
     size_t host_stage_bytes = 0;
     cudaEvent_t stage_ev[2] = {nullptr, nullptr};
@@ -195,11 +205,15 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     P.merge_items = ctx->r0_merge_items;
     P.class_streams = ctx->class_streams;
     P.split = ctx->allow_split;
+    P.r0_variant = ctx->r0_variant;
+    P.wide_stages = ctx->wide_stages;
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
     if (tu != ctx->tuned.end()) {
         P.pairs_per_job = tu->second[0];
         P.merge_items = tu->second[1];
         P.class_streams = tu->second[2];
+        P.r0_variant = tu->second[3];
+        P.wide_stages = tu->second[4];
     }
     const int n = (int)Ms.size();
     long long f = 0, s = 0;
@@ -212,7 +226,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         if (pd.Np > MAX_NP) return fail(ctx, BPMAX_EINVAL, "strand-2 length %d > %d is not supported", Ns[p], MAX_NP);
         pd.F_off = f;
         f = align64(f + (long long)Ms[p] * (Ms[p] + 1) / 2 * cell_floats(pd.Np));
-        if (pd.Np > MAX_SMALL_NP) P.any_wide = true;
+        if (pd.Np > WIDE_TILE_MAX_NP) P.any_large = true;
         pd.S1_off = s;
         s = align64(s + (long long)Ms[p] * Ms[p]);
         pd.S2_off = s;
@@ -259,7 +273,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 // offset d-1-w) fall in the same pair chunk
                 const int NB = np / 8, G = R0_TAB_ITEMS[NB];
                 const long long P2 = (d + 1) / 2;  // offset pairs per cell
-                const long long resident = (long long)std::max(1, ctx->r0_occ[NB]) * ctx->sms;
+                const long long resident = (long long)std::max(1, ctx->r0_occ_v[P.r0_variant][NB]) * ctx->sms;
                 const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(P.pairs_per_job, qmin);
                 // Offset pair 0 (offsets 0 and d-1) is the only one that reads diagonal d-1. In a plan
                 // of one width class, where one iteration holds at most 2 items, it becomes its own
@@ -284,6 +298,39 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                                 P.r0_jobs.push_back(R0Job{p, i1, (int)c0, (int)std::min(c0 + q, P2)});
                 rl.count = (int)P.r0_jobs.size() - rl.first;
                 P.r0_launches.push_back(rl);
+                continue;
+            }
+            if (np <= WIDE_TILE_MAX_NP) {
+                // tile images: one job per output tile (BI, BJ) of a cell and chunk of k1 offset pairs,
+                // each tile's chunk sized so that jobs cost about the same: cost per offset pair in
+                // warp task steps of both of its items, DD 3.3, DA and DB 12, F 16 per item
+                const int NT = np / 64;
+                const long long P2 = (d + 1) / 2;
+                const long long resident = (long long)std::max(1, ctx->wide_occ[P.wide_stages]) * ctx->sms;
+                std::vector<std::pair<double, int>> tiles;  // (cost per offset pair, BI << 8 | BJ)
+                double per_pair = 0;
+                for (int BI = 0; BI < NT; ++BI)
+                    for (int BJ = BI; BJ < NT; ++BJ) {
+                        const double c = BI == BJ ? 2 * 3.3 : 2 * (24.0 + 16.0 * (BJ - BI - 1));
+                        tiles.push_back({c, BI << 8 | BJ});
+                        per_pair += c;
+                    }
+                std::stable_sort(tiles.begin(), tiles.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+                const double total = (double)cells * P2 * per_pair;
+                const double target = std::max(total / (3.0 * resident), 4.0 * 16.0);
+                const size_t first = P.r0w_jobs.size();
+                for (const auto &t : tiles) {
+                    const long long q = std::max(1LL, std::min(P2, (long long)std::llround(target / t.first)));
+                    for (long long c0 = 0; c0 < P2; c0 += q)
+                        for (int p = 0; p < n; ++p)
+                            if (P.pairs[p].Np == np && Ms[p] > d)
+                                for (int i1 = 0; i1 < Ms[p] - d; ++i1)
+                                    P.r0w_jobs.push_back(R0JobW{p, i1, t.second, (int)c0, (int)std::min(c0 + q, P2)});
+                }
+                // jobs of the same offset pairs together (both uses of a table meet in L2), heavy tiles first
+                std::stable_sort(P.r0w_jobs.begin() + first, P.r0w_jobs.end(),
+                                 [](const R0JobW &a, const R0JobW &b) { return a.p0 < b.p0; });
+                P.r0_launches.push_back(Plan::Launch{d, np, (int)first, (int)(P.r0w_jobs.size() - first)});
                 continue;
             }
             const int nbk = np / 64;
@@ -320,13 +367,30 @@ void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
         (const float *)ctx->FT.p, (const float *)ctx->S.p, L.d);
 }
 
+template <int STAGES>
+void launch_r0_wide_t(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
+{
+    const int grid = std::min(L.count, std::max(1, ctx->wide_occ[STAGES]) * ctx->sms);
+    r0_wide_kernel<STAGES><<<grid, WideCfg<STAGES>::THREADS, WideCfg<STAGES>::SMEM, s>>>(
+        (const R0JobW *)ctx->r0wjobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
+        wait_ctl(ctx));
+}
+
+void launch_r0_wide(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaStream_t s)
+{
+    if (P.wide_stages == 3)
+        launch_r0_wide_t<3>(ctx, L, s);
+    else
+        launch_r0_wide_t<2>(ctx, L, s);
+}
+
 void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
     if (L.np <= FIN_WIDE_MAX_NP) {
         constexpr int WW = FIN_WIDE_THREADS / 32;
         finalize_wide_kernel<<<L.count + (L.s1_count + WW - 1) / WW, FIN_WIDE_THREADS, fin_wide_smem(L.np), s>>>(
             (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first,
-            L.s1_count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
+            L.s1_count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p,
             (const uint8_t *)ctx->bases.p, ctx->W, L.d);
         return;
     }
@@ -337,14 +401,23 @@ void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
         (const uint8_t *)ctx->bases.p, ctx->W, L.d);
 }
 
-template <int NB>
-void launch_r0(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
+template <int NB, int V>
+void launch_r0_v(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
-    using C = R0Cfg<NB>;
-    const int grid = std::min(L.count, std::max(1, ctx->r0_occ[NB]) * ctx->sms);  // resident CTAs; each loops over jobs
-    r0_kernel<NB><<<grid, C::THREADS, C::SMEM, s>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
-                                                              (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
-                                                              wait_ctl(ctx));
+    using C = R0Cfg<NB, V>;
+    const int grid = std::min(L.count, std::max(1, ctx->r0_occ_v[V][NB]) * ctx->sms);  // resident CTAs; each loops over jobs
+    r0_kernel<NB, V><<<grid, C::THREADS, C::SMEM, s>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
+                                                       (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
+                                                       wait_ctl(ctx));
+}
+
+template <int NB>
+void launch_r0(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaStream_t s)
+{
+    if (P.r0_variant == 1)
+        launch_r0_v<NB, 1>(ctx, L, s);
+    else
+        launch_r0_v<NB, 0>(ctx, L, s);
 }
 
 template <int NB, int T>
@@ -373,8 +446,11 @@ void launch_r0only_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     const float *vals = (const float *)ctx->r0vals.p;
     switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
     case 0:
-        r0only_finalize_wide_kernel<<<dim3(L.count, L.np / R0ONLY_TILE), 256, 0, s>>>(jobs, pd, (float *)ctx->F.p,
-                                                                                     (float *)ctx->FT.p, vals, L.d);
+        if (L.np <= WIDE_TILE_MAX_NP)
+            r0only_finalize_tile_kernel<<<L.count, 256, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d);
+        else
+            r0only_finalize_wide_kernel<<<dim3(L.count, L.np / R0ONLY_TILE), 256, 0, s>>>(jobs, pd, (float *)ctx->F.p,
+                                                                                         (float *)ctx->FT.p, vals, L.d);
         break;
     case 1: r0only_finalize_small_kernel<8><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
     case 2: r0only_finalize_small_kernel<16><<<L.count, 128, 0, s>>>(jobs, pd, (float *)ctx->F.p, vals, L.d); break;
@@ -391,13 +467,21 @@ template <int NB>
 int set_smem_attr(bpmax_ctx *ctx)
 {
     CK(cudaFuncSetAttribute(r0_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM));
+    CK(cudaFuncSetAttribute(r0_kernel<NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB, 1>::SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ_v[1][NB], r0_kernel<NB, 1>, R0Cfg<NB, 1>::THREADS,
+                                                     R0Cfg<NB, 1>::SMEM));
     CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)FinShape<8 * NB>::SMEM));
     if constexpr (8 * NB >= 48)
         CK(cudaFuncSetAttribute(finalize_small_kernel<8 * NB, FIN_BULK_THREADS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FinShape<8 * NB, FIN_BULK_THREADS>::SMEM));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ[NB], r0_kernel<NB>, R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ_v[0][NB], r0_kernel<NB>, R0Cfg<NB>::THREADS,
+                                                     R0Cfg<NB>::SMEM));
     if (NB == 8) {
+        CK(cudaFuncSetAttribute(r0_wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideCfg<2>::SMEM));
+        CK(cudaFuncSetAttribute(r0_wide_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideCfg<3>::SMEM));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->wide_occ[2], r0_wide_kernel<2>, 128, WideCfg<2>::SMEM));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->wide_occ[3], r0_wide_kernel<3>, 128, WideCfg<3>::SMEM));
         CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideShape::SMEM));
         CK(cudaFuncSetAttribute(finalize_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)fin_wide_smem(FIN_WIDE_MAX_NP)));
@@ -502,15 +586,20 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
             {
                 ProfScope ps(ctx, kp, 1);
                 switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-                case 0: launch_r0_large(ctx, L, st); break;
-                case 1: launch_r0<1>(ctx, L, st); break;
-                case 2: launch_r0<2>(ctx, L, st); break;
-                case 3: launch_r0<3>(ctx, L, st); break;
-                case 4: launch_r0<4>(ctx, L, st); break;
-                case 5: launch_r0<5>(ctx, L, st); break;
-                case 6: launch_r0<6>(ctx, L, st); break;
-                case 7: launch_r0<7>(ctx, L, st); break;
-                default: launch_r0<8>(ctx, L, st); break;
+                case 0:
+                    if (L.np <= WIDE_TILE_MAX_NP)
+                        launch_r0_wide(ctx, P, L, st);
+                    else
+                        launch_r0_large(ctx, L, st);
+                    break;
+                case 1: launch_r0<1>(ctx, P, L, st); break;
+                case 2: launch_r0<2>(ctx, P, L, st); break;
+                case 3: launch_r0<3>(ctx, P, L, st); break;
+                case 4: launch_r0<4>(ctx, P, L, st); break;
+                case 5: launch_r0<5>(ctx, P, L, st); break;
+                case 6: launch_r0<6>(ctx, P, L, st); break;
+                case 7: launch_r0<7>(ctx, P, L, st); break;
+                default: launch_r0<8>(ctx, P, L, st); break;
                 }
             }
             if (split && L.part == 0) {
@@ -569,11 +658,12 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
 {
     int st;
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
-    const std::array<int, 3> want = tu != ctx->tuned.end()
-                                        ? tu->second
-                                        : std::array<int, 3>{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams};
+    const Tuned want = tu != ctx->tuned.end() ? tu->second
+                                              : Tuned{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams,
+                                                      ctx->r0_variant, ctx->wide_stages};
     const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
-                             ctx->plan.class_streams == want[2];
+                             ctx->plan.class_streams == want[2] && ctx->plan.r0_variant == want[3] &&
+                             ctx->plan.wide_stages == want[4];
     if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only &&
           ctx->plan.split == ctx->allow_split)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
@@ -589,18 +679,22 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
             for (auto &e : P.diag_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
         if ((st = ensure(ctx, ctx->F, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
-        if (P.any_wide && (st = ensure(ctx, ctx->FT, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
+        if (P.any_large && (st = ensure(ctx, ctx->FT, P.F_floats * sizeof(float))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->errflag, sizeof(int))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->S, P.S_floats * sizeof(float))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->bases, P.bases_bytes + 16)) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->pairs, P.pairs.size() * sizeof(PairDesc))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->r0jobs, P.r0_jobs.size() * sizeof(R0Job))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->r0ljobs, P.r0l_jobs.size() * sizeof(R0JobL))) != BPMAX_OK) return st;
+        if ((st = ensure(ctx, ctx->r0wjobs, P.r0w_jobs.size() * sizeof(R0JobW))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->celljobs, P.cell_jobs.size() * sizeof(CellJob))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->scores, P.pairs.size() * sizeof(float))) != BPMAX_OK) return st;
         CK(cudaMemcpyAsync(ctx->pairs.p, P.pairs.data(), P.pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, ctx->stream));
         if (!P.r0_jobs.empty())
             CK(cudaMemcpyAsync(ctx->r0jobs.p, P.r0_jobs.data(), P.r0_jobs.size() * sizeof(R0Job), cudaMemcpyHostToDevice, ctx->stream));
+        if (!P.r0w_jobs.empty())
+            CK(cudaMemcpyAsync(ctx->r0wjobs.p, P.r0w_jobs.data(), P.r0w_jobs.size() * sizeof(R0JobW), cudaMemcpyHostToDevice,
+                               ctx->stream));
         if (!P.r0l_jobs.empty())
             CK(cudaMemcpyAsync(ctx->r0ljobs.p, P.r0l_jobs.data(), P.r0l_jobs.size() * sizeof(R0JobL), cudaMemcpyHostToDevice,
                                ctx->stream));
@@ -826,7 +920,7 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
     for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs,
-                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->celljobs, &ctx->scores, &ctx->conv, &ctx->errflag,
+                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->r0wjobs, &ctx->celljobs, &ctx->scores, &ctx->conv, &ctx->errflag,
                       &ctx->r0vals})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
@@ -1131,6 +1225,14 @@ int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value)
     case BPMAX_TUNE_INJECT_WAIT_TIMEOUT:
         ctx->inject_wait_timeout = value != 0;
         break;
+    case BPMAX_TUNE_WIDE_STAGES:
+        if (value != 2 && value != 3) return fail(ctx, BPMAX_EINVAL, "tile-product stages must be 2 or 3");
+        ctx->wide_stages = (int)value;
+        break;
+    case BPMAX_TUNE_R0_VARIANT:
+        if (value != 0 && value != 1) return fail(ctx, BPMAX_EINVAL, "product shape variant must be 0 or 1");
+        ctx->r0_variant = (int)value;
+        break;
     default: return fail(ctx, BPMAX_EINVAL, "unknown tuning key %d", key);
     }
     return BPMAX_OK;
@@ -1145,6 +1247,8 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value)
     case BPMAX_TUNE_CLASS_STREAMS: *value = ctx->class_streams; break;
     case BPMAX_TUNE_WAIT_LIMIT_US: *value = (long)(ctx->wait_ns / 1000ULL); break;
     case BPMAX_TUNE_INJECT_WAIT_TIMEOUT: *value = ctx->inject_wait_timeout ? 1 : 0; break;
+    case BPMAX_TUNE_WIDE_STAGES: *value = ctx->wide_stages; break;
+    case BPMAX_TUNE_R0_VARIANT: *value = ctx->r0_variant; break;
     default: return BPMAX_EINVAL;
     }
     return BPMAX_OK;
@@ -1162,39 +1266,54 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
     }
     const std::vector<int> key = shape_key(vm, vn);
     ctx->tuned.erase(key);
-    const int saved[3] = {ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams};
+    const Tuned saved{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams, ctx->r0_variant, ctx->wide_stages};
     std::set<int> classes;
-    for (int n : vn) classes.insert(padded_width(n));
-    const int jobs_cand[] = {8, 32, 1 << 20}, merge_cand[] = {1, 4}, streams_cand[] = {1, 0};
+    bool small = false, tiled = false;
+    for (int n : vn) {
+        const int np = padded_width(n);
+        classes.insert(np);
+        small = small || np <= MAX_SMALL_NP;
+        tiled = tiled || is_tiled(np);
+    }
     float best_t = -1.f;
-    std::array<int, 3> best_cfg{saved[0], saved[1], saved[2]};
+    Tuned best_cfg = saved;
     int st = BPMAX_OK;
+    auto try_cfg = [&](const Tuned &c) {
+        ctx->r0_pairs_per_job = c[0];
+        ctx->r0_merge_items = c[1];
+        ctx->class_streams = c[2];
+        ctx->r0_variant = c[3];
+        ctx->wide_stages = c[4];
+        float t = -1.f;
+        for (int r = 0; r < 1 + std::max(1, trials) && st == BPMAX_OK; ++r) {  // first run captures the graph
+            st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
+            if (st == BPMAX_OK && r > 0 && (t < 0 || ctx->last_ms < t)) t = ctx->last_ms;
+        }
+        if (st == BPMAX_OK && (best_t < 0 || t < best_t)) {
+            best_t = t;
+            best_cfg = c;
+        }
+    };
+    // the schedule knobs with the default kernel shapes, then the kernel shapes with the best schedule
+    const int jobs_cand[] = {8, 32, 1 << 20}, merge_cand[] = {1, 4}, streams_cand[] = {1, 0};
     for (int sc : streams_cand) {
         if (sc == 0 && classes.size() < 2) continue;  // one class: the stream setting changes nothing
         for (int jc : jobs_cand)
-            for (int mc : merge_cand) {
-                ctx->r0_pairs_per_job = jc;
-                ctx->r0_merge_items = mc;
-                ctx->class_streams = sc;
-                float t = -1.f;
-                for (int r = 0; r < 1 + std::max(1, trials) && st == BPMAX_OK; ++r) {  // first run captures the graph
-                    st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
-                    if (st == BPMAX_OK && r > 0 && (t < 0 || ctx->last_ms < t)) t = ctx->last_ms;
-                }
-                if (st != BPMAX_OK) break;
-                if (best_t < 0 || t < best_t) {
-                    best_t = t;
-                    best_cfg = {jc, mc, sc};
-                }
-            }
+            for (int mc : merge_cand)
+                if (st == BPMAX_OK) try_cfg(Tuned{jc, mc, sc, 0, 2});
     }
+    const Tuned sched = best_cfg;
+    if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4]});
+    if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3});
     ctx->r0_pairs_per_job = saved[0];
     ctx->r0_merge_items = saved[1];
     ctx->class_streams = saved[2];
+    ctx->r0_variant = saved[3];
+    ctx->wide_stages = saved[4];
     if (st != BPMAX_OK) return st;
     ctx->tuned[key] = best_cfg;
     if (best)
-        for (int k = 0; k < 3; ++k) best[k] = best_cfg[k];
+        for (int k = 0; k < 5; ++k) best[k] = best_cfg[k];
     if (best_ms) *best_ms = best_t;
     return BPMAX_OK;
 }

@@ -19,8 +19,9 @@
 //       chunks (the pads spread the product kernel's shared loads over the bank groups). Inside
 //       diagonal blocks the entries below the diagonal are -inf except the subdiagonal, which
 //       holds S1 of the cell; padding rows/columns (>= N) are -inf.
-//     Np > 64 (a multiple of 64): row-major Np x Np with -inf outside the logical triangle and S1
-//       on the subdiagonal, plus FT, the same table transposed (bpmax_kernels_large.cuh).
+//     64 < Np <= 320 (a multiple of 64): tile images (below);
+//     Np > 320: row-major Np x Np with -inf outside the logical triangle and S1 on the
+//       subdiagonal, plus FT, the same table transposed (bpmax_kernels_large.cuh).
 //   S1[M][M], S2[Np][Np] single-strand tables (S2 over the reversed strand 2)
 #pragma once
 #include <cstdint>
@@ -81,17 +82,67 @@ __host__ __device__ __forceinline__ long long cell_index(int M, int i1, int j1)
 
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
 
+// ------------------------------------------------------------------------------------------
+// Tile images: inner tables of width 64 < Np <= WIDE_TILE_MAX_NP (Np = 64 * NT) are stored per
+// outer cell as the upper triangle of NT x NT tiles of 64 x 64 in row-major tile-triangle order. A
+// diagonal tile is a width-64 cell image (above); an off-diagonal ("dense") tile holds all 64 of
+// its 8x8 blocks in block columns at WIDE_DENSE_COLBASE (wide_tables.inc), each column closed by a
+// halo piece: row 0 of block (0, bj) of the tile below, the row after the tile, so the row-shifted
+// operand of any tile is one image. Rows and columns >= N are -inf.
+// Wider tables (Np > WIDE_TILE_MAX_NP) are row-major with a transposed copy (bpmax_kernels_large.cuh).
+// ------------------------------------------------------------------------------------------
+#include "wide_tables.inc"
+
+constexpr int WIDE_TILE_MAX_NP = 320;                     // widest table stored as tile images
+constexpr int WIDE_DIAG_CHUNKS = R0_TAB_COLBASE[8][8];    // diagonal tile image (width-64 cell image)
+constexpr int WIDE_DENSE_CHUNKS = WIDE_DENSE_COLBASE[8];  // dense tile image
+
+__host__ __device__ __forceinline__ bool is_tiled(int Np) { return Np > 64 && Np <= WIDE_TILE_MAX_NP; }
+
+// float offset of tile (I, J), I <= J, inside a cell's table of NT x NT tiles
+__host__ __device__ __forceinline__ long long wide_tile_off(int NT, int I, int J)
+{
+    const long long SD = 4LL * WIDE_DIAG_CHUNKS, SQ = 4LL * WIDE_DENSE_CHUNKS;
+    long long o = (long long)I * SD + SQ * ((long long)I * (NT - 1) - (long long)I * (I - 1) / 2);
+    if (J > I) o += SD + (long long)(J - I - 1) * SQ;
+    return o;
+}
+__host__ __device__ __forceinline__ long long wide_cell_floats(int NT)
+{
+    return (long long)NT * 4 * WIDE_DIAG_CHUNKS + (long long)NT * (NT - 1) / 2 * 4 * WIDE_DENSE_CHUNKS;
+}
+
+#ifdef __CUDA_ARCH__
+#define WIDE_DENSE_CB(c) c_wide_dense_colbase[c]
+#else
+#define WIDE_DENSE_CB(c) WIDE_DENSE_COLBASE[c]
+#endif
+
+// float offset, inside a cell's table of NT x NT tiles, of the stored entry (r, c) with r <= c
+__host__ __device__ __forceinline__ long long wide_pos(int NT, int r, int c)
+{
+    const int I = r >> 6, J = c >> 6, lr = r & 63, lc = c & 63, bi = lr >> 3, bj = lc >> 3;
+    const int cb = I == J ? IMG_COLBASE(8, bj) : WIDE_DENSE_CB(bj);
+    return wide_tile_off(NT, I, J) + 4 * (cb + 17 * bi) + 8 * (lr & 7) + (lc & 7);
+}
+
 // floats per stored cell table of a pair
 __host__ __device__ __forceinline__ long long cell_floats(int Np)
 {
-    return Np <= 64 ? 4LL * IMG_COLBASE(Np >> 3, Np >> 3) : (long long)Np * Np;
+    if (Np <= 64) return 4LL * IMG_COLBASE(Np >> 3, Np >> 3);
+    if (Np <= WIDE_TILE_MAX_NP) return wide_cell_floats(Np >> 6);
+    return (long long)Np * Np;
 }
 
 // F(cell)[r][c] for any r, c < Np (entries below the diagonal as the tables define them)
 __device__ __forceinline__ float f_value(const PairDesc &pd, const float *__restrict__ F, long long cell, int r, int c)
 {
     const float *C = F + pd.F_off + cell * cell_floats(pd.Np);
-    if (pd.Np > 64) return C[(long long)r * pd.Np + c];
+    if (pd.Np > WIDE_TILE_MAX_NP) return C[(long long)r * pd.Np + c];
+    if (pd.Np > 64) {
+        if (r > c) return r == c + 1 ? C[4 * 17 + 7] : NEG_INF;  // S1 piece of column 0 of tile (0, 0)
+        return C[wide_pos(pd.Np >> 6, r, c)];
+    }
     const int NB = pd.Np >> 3, BI = r >> 3, BJ = c >> 3;
     if (BI > BJ) return r == c + 1 ? C[4 * 17 + 7] : NEG_INF;  // S1 piece of column 0
     return C[4 * (c_img_colbase[NB][BJ] + 17 * BI) + 8 * (r & 7) + (c & 7)];

@@ -366,17 +366,18 @@ finalize_large_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
 }
 
 // ------------------------------------------------------------------------------------------
-// Finalize for 64 < Np <= FIN_WIDE_MAX_NP: same candidates and same results as
-// finalize_large_kernel, with the inner wavefront pushed forward in shared memory. The CTA keeps
-// the cell's inner table diagonal-major and triangular, D[e][i2] = F[i2][i2+e] (T(Np) floats),
-// each open entry holding its running maximum. When inner diagonal e is final, every open cell
-// (e2 > e) takes its two candidates that read diagonal e,
+// Finalize for 64 < Np <= FIN_WIDE_MAX_NP (tables stored as tile images, bpmax_kernels.cuh): same
+// candidates and same results as finalize_large_kernel, with the inner wavefront pushed forward in
+// shared memory. The CTA keeps the cell's inner table diagonal-major and triangular,
+// D[e][i2] = F[i2][i2+e] (T(Np) floats), each open entry holding its running maximum. When inner
+// diagonal e is final, every open cell (e2 > e) takes its two candidates that read diagonal e,
 //   R1 with k2 = i2+e:    F[i2][i2+e] + S2(i2+e+1, j2)
 //   R2 with k2 = j2-e-1:  S2(i2, j2-e-1) + F[j2-e][j2]
 // and the cells of diagonal e+1 become final after SW2. Warp w takes the diagonals e2 = e+1+w,
 // e+1+w+32, ...; its lanes take consecutive i2, so both S2 reads are one coalesced line of the
-// diagonal-major copy and the D reads are conflict-free. One CTA barrier per inner diagonal. F
-// and FT are written once, at the end, row by row.
+// diagonal-major copy and the D reads are conflict-free. One CTA barrier per inner diagonal. The
+// tile images (blocks, S1 pieces of the diagonal tiles, halo pieces of the dense tiles) are written
+// once, at the end, four columns of one block row per thread and step.
 // CTAs after the first njobs compute S1 on diagonal d+1, one warp per cell.
 // ------------------------------------------------------------------------------------------
 constexpr int FIN_WIDE_THREADS = 1024;
@@ -386,8 +387,8 @@ __host__ __device__ constexpr size_t fin_wide_smem(int Np) { return (size_t)Np *
 
 __global__ void __launch_bounds__(FIN_WIDE_THREADS)
 finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
-                     const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
-                     float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
+                     const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ S,
+                     const uint8_t *__restrict__ bases, Weights W, int d)
 {
     constexpr int NT = FIN_WIDE_THREADS, WARPS = NT / 32;
     extern __shared__ __align__(16) float fwd[];
@@ -412,10 +413,9 @@ finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob 
     }
     const CellJob job = jobs[blockIdx.x];
     const PairDesc pd = pairs[job.pair];
-    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1, j1 = i1 + d;
-    const long long tile = (long long)Np * Np;
-    float *Fc = F + pd.F_off + cell_index(M, i1, j1) * tile;
-    float *FTc = FT + pd.F_off + cell_index(M, i1, j1) * tile;
+    const int M = pd.M, N = pd.N, Np = pd.Np, NTL = Np >> 6, i1 = job.i1, j1 = i1 + d;
+    const long long CELL = wide_cell_floats(NTL);
+    float *Fc = F + pd.F_off + cell_index(M, i1, j1) * CELL;
     const float *S1 = S + pd.S1_off;
     const float *S2 = S + pd.S2_off;
     const float *S2D = S + pd.S2d_off;
@@ -430,7 +430,8 @@ finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob 
     for (int q = tid; q < Np * Np; q += NT) {
         const int r = q / Np, c = q % Np;
         if (r <= c && c < N)
-            D[drow(Np, c - r) + r] = (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(Fc[q], s1v + S2[q]);
+            D[drow(Np, c - r) + r] =
+                (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(Fc[wide_pos(NTL, r, c)], s1v + S2[q]);
     }
     __syncthreads();
     for (int e = 0; e + 1 < N; ++e) {
@@ -449,20 +450,52 @@ finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob 
         }
         __syncthreads();
     }
-    // F and FT, row by row: the logical triangle, S1(i1,j1) on the subdiagonal, -inf elsewhere;
-    // SW1 candidate of cell (i1-1, j1+1), whose table nothing else has written yet
+    // the tile images: the logical triangle, S1(i1,j1) on the subdiagonal, -inf elsewhere; the S1
+    // pieces of the diagonal tiles and the halo pieces of the dense ones; and the SW1 candidate of
+    // cell (i1-1, j1+1), whose table nothing else has written yet (blocks only)
     const bool push = i1 >= 1 && j1 + 1 < M && d + 2 >= 4;
     const float wp = push ? score_w(wsh, s1[i1 - 1], s1[j1 + 1]) : 0.0f;
-    float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * tile : nullptr;
-    for (int q = tid; q < Np * Np; q += NT) {
-        const int r = q / Np, c = q % Np;
-        const bool vf = r <= c && c < N, vt = c <= r && r < N;
-        const float f = vf ? D[drow(Np, c - r) + r] : (r == c + 1 ? s1v : NEG_INF);
-        const float t = vt ? D[drow(Np, r - c) + c] : (c == r + 1 ? s1v : NEG_INF);  // F[c][r]
-        Fc[q] = f;
-        FTc[q] = t;
-        if (push) Fn[q] = vf ? f + wp : 0.0f;
-    }
+    float *Fn = push ? F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * CELL : nullptr;
+    auto val = [&](int r, int c) {  // stored value of entry (r, c), r <= c + 1
+        return (r <= c && c < N) ? D[drow(Np, c - r) + r] : (r == c + 1 ? s1v : NEG_INF);
+    };
+    for (int I = 0; I < NTL; ++I)
+        for (int J = I; J < NTL; ++J) {
+            const long long to = wide_tile_off(NTL, I, J);
+            const int nblk = I == J ? 36 : 64;
+            for (int q4 = tid; q4 < nblk * 16 + 16; q4 += NT) {
+                if (q4 >= nblk * 16) {  // the closing piece of block column bj: S1 piece or halo piece
+                    const int bj = (q4 - nblk * 16) >> 1, h = q4 & 1;
+                    const int cb = I == J ? c_img_colbase[8][bj] : c_wide_dense_colbase[bj];
+                    float v[4];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
+                        v[t] = I == J ? ((h == 1 && t == 3) ? s1v : NEG_INF) : val(64 * I + 64, 64 * J + 8 * bj + 4 * h + t);
+                    *reinterpret_cast<float4 *>(Fc + to + 4 * (cb + 17 * (I == J ? bj + 1 : 8)) + 4 * h) =
+                        make_float4(v[0], v[1], v[2], v[3]);
+                    continue;
+                }
+                int bi, bj;
+                if (I == J) {
+                    blk_decode(8, q4 >> 4, bi, bj);
+                } else {
+                    bi = (q4 >> 4) & 7;
+                    bj = q4 >> 7;
+                }
+                const int r = 64 * I + 8 * bi + ((q4 & 15) >> 1), c0 = 64 * J + 8 * bj + 4 * (q4 & 1);
+                float v[4], u[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int c = c0 + t;
+                    v[t] = val(r, c);
+                    u[t] = (r <= c && c < N) ? v[t] + wp : 0.0f;
+                }
+                const long long o = to + 4 * ((I == J ? c_img_colbase[8][bj] : c_wide_dense_colbase[bj]) + 17 * bi) +
+                                    4 * (q4 & 15);
+                if (push) *reinterpret_cast<float4 *>(Fn + o) = make_float4(u[0], u[1], u[2], u[3]);
+                *reinterpret_cast<float4 *>(Fc + o) = make_float4(v[0], v[1], v[2], v[3]);
+            }
+        }
 }
 
 }  // namespace bpmax

@@ -66,7 +66,10 @@ __host__ __device__ __forceinline__ int r0_item_offset(const R0Job &j, int d, in
     return (n & 1) ? d - 1 - p : p;
 }
 
-template <int NB>
+// Shape variant V of the kernel for width class NB (a tunable of the schedule; results identical):
+//   V = 0  three CTAs per SM (four for the 96-thread NB = 7), 168 registers, a 2..4-stage ring;
+//   V = 1  two CTAs per SM (three below 128 threads), up to 255 registers, a ring of up to 6 stages.
+template <int NB, int V = 0>
 struct R0Cfg {
     static constexpr int NP = 8 * NB;
     static constexpr int THREADS = R0_TAB_THREADS[NB];
@@ -79,10 +82,15 @@ struct R0Cfg {
     static constexpr int RED_WORDS = 65 * NBLK;             // job-merge tile, one 8x8 block per 65 words
     // shared-memory budget of the stages: 3 CTAs per SM; 4 for the 96-thread NB = 7 CTAs (their
     // registers allow it, and 12 resident warps beat a fourth stage)
-    static constexpr int STAGE_BUDGET = (NB == 7 ? 55 : 75) * 1024 - 4 * RED_WORDS - 4 * NBLK - 64;
-    static constexpr int STAGES = STAGE_BYTES * 4 <= STAGE_BUDGET ? 4 : (STAGE_BYTES * 3 <= STAGE_BUDGET ? 3 : 2);
+    static constexpr int STAGE_BUDGET =
+        (V == 1 ? (THREADS <= 96 ? 74 : 112) : (NB == 7 ? 55 : 75)) * 1024 - 4 * RED_WORDS - 4 * NBLK - 64;
+    static constexpr int MAX_STAGES = V == 1 ? 6 : 4;
+    static constexpr int STAGES = STAGE_BYTES * MAX_STAGES <= STAGE_BUDGET
+                                      ? MAX_STAGES
+                                      : (STAGE_BYTES * 4 <= STAGE_BUDGET ? 4 : (STAGE_BYTES * 3 <= STAGE_BUDGET ? 3 : 2));
     static constexpr int ITEM_TX = 2 * IMG * 16;            // bytes landing per item
-    static constexpr int MINB = THREADS <= 64 ? 6 : (THREADS <= 96 ? 4 : 3);
+    static constexpr int MINB = V == 1 ? (THREADS <= 64 ? 4 : (THREADS <= 96 ? 3 : 2))
+                                       : (THREADS <= 64 ? 6 : (THREADS <= 96 ? 4 : 3));
     // shared memory: stages, merge tile, block offsets, one mbarrier per stage (byte offsets)
     static constexpr int OFF_RED = STAGES * STAGE_BYTES;
     static constexpr int OFF_DST = OFF_RED + 4 * RED_WORDS;
@@ -209,12 +217,12 @@ __device__ __forceinline__ void r0_task(const float *__restrict__ As, const floa
     }
 }
 
-template <int NB>
-__global__ void __launch_bounds__(R0Cfg<NB>::THREADS, R0Cfg<NB>::MINB)
+template <int NB, int V = 0>
+__global__ void __launch_bounds__(R0Cfg<NB, V>::THREADS, R0Cfg<NB, V>::MINB)
 r0_kernel(const R0Job *__restrict__ jobs, int njobs, const PairDesc *__restrict__ pairs, float *__restrict__ F, int d,
           WaitCtl ctl)
 {
-    using C = R0Cfg<NB>;
+    using C = R0Cfg<NB, V>;
     constexpr int S = C::STAGES;
     constexpr long long CELL = 4LL * C::IMG;
     extern __shared__ __align__(128) float r0sm[];

@@ -60,7 +60,58 @@ __global__ void __launch_bounds__(128) r0only_finalize_small_kernel(const CellJo
     }
 }
 
-// Row-major tables and their transposes (Np > 64): CTA (blockIdx.x, blockIdx.y) writes the 32-row
+// Tile images (64 < Np <= WIDE_TILE_MAX_NP): one CTA per outer cell of diagonal d rewrites every
+// block of every tile with the base values and -inf where the full fill writes S1, and writes the
+// closing pieces (S1 pieces of the diagonal tiles: -inf; halo pieces of the dense tiles: the row
+// after the tile, by the same rule). The rule is idempotent, so reading an entry another thread
+// has already rewritten gives the same value.
+__global__ void __launch_bounds__(256) r0only_finalize_tile_kernel(const CellJob *__restrict__ jobs,
+                                                                  const PairDesc *__restrict__ pairs,
+                                                                  float *__restrict__ F,
+                                                                  const float *__restrict__ vals, int d)
+{
+    const CellJob job = jobs[blockIdx.x];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, NT = pd.Np >> 6, i1 = job.i1;
+    float *Fc = F + pd.F_off + cell_index(M, i1, i1 + d) * wide_cell_floats(NT);
+    const float *v1 = vals, *v2 = vals + M;
+    auto val = [&](int r, int c) {
+        return !(r <= c && c < N) ? NEG_INF : (d == 0 ? v2[r] : (r == c ? v1[i1] : Fc[wide_pos(NT, r, c)]));
+    };
+    for (int I = 0; I < NT; ++I)
+        for (int J = I; J < NT; ++J) {
+            const long long to = wide_tile_off(NT, I, J);
+            const int nblk = I == J ? 36 : 64;
+            for (int q4 = threadIdx.x; q4 < nblk * 16 + 16; q4 += blockDim.x) {
+                if (q4 >= nblk * 16) {
+                    const int bj = (q4 - nblk * 16) >> 1, h = q4 & 1;
+                    float v[4];
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) v[t] = I == J ? NEG_INF : val(64 * I + 64, 64 * J + 8 * bj + 4 * h + t);
+                    const int cb = I == J ? c_img_colbase[8][bj] : c_wide_dense_colbase[bj];
+                    *reinterpret_cast<float4 *>(Fc + to + 4 * (cb + 17 * (I == J ? bj + 1 : 8)) + 4 * h) =
+                        make_float4(v[0], v[1], v[2], v[3]);
+                    continue;
+                }
+                int bi, bj;
+                if (I == J) {
+                    blk_decode(8, q4 >> 4, bi, bj);
+                } else {
+                    bi = (q4 >> 4) & 7;
+                    bj = q4 >> 7;
+                }
+                const int r = 64 * I + 8 * bi + ((q4 & 15) >> 1), c0 = 64 * J + 8 * bj + 4 * (q4 & 1);
+                float v[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) v[t] = val(r, c0 + t);
+                const long long o = to + 4 * ((I == J ? c_img_colbase[8][bj] : c_wide_dense_colbase[bj]) + 17 * bi) +
+                                    4 * (q4 & 15);
+                *reinterpret_cast<float4 *>(Fc + o) = make_float4(v[0], v[1], v[2], v[3]);
+            }
+        }
+}
+
+// Row-major tables and their transposes (Np > WIDE_TILE_MAX_NP): CTA (blockIdx.x, blockIdx.y) writes the 32-row
 // band blockIdx.y of cell blockIdx.x of diagonal d, one 32 x 32 tile at a time, and the matching
 // column band of the transpose through a shared tile (coalesced reads and writes on both sides).
 constexpr int R0ONLY_TILE = 32;

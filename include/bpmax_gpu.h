@@ -119,23 +119,34 @@ int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s,
  *   BPMAX_TUNE_INJECT_WAIT_TIMEOUT  1: the next fill call (only that one) runs its product kernels
  *                                without issuing any operand copy, so their first waits run out with
  *                                no copy in flight; the call returns BPMAX_ETIMEOUT and later calls
- *                                are unaffected. A test of the timeout path; 0 otherwise. */
+ *                                are unaffected. A test of the timeout path; 0 otherwise.
+ *   BPMAX_TUNE_WIDE_STAGES       shared-memory stages of the product kernel for strand-2 lengths 65..320
+ *                                (2: three CTAs per SM; 3: two CTAs per SM with a deeper copy ring)
+ *   BPMAX_TUNE_R0_VARIANT        shape of the product kernel for strand-2 lengths <= 64 (0: three CTAs
+ *                                per SM, 168 registers, 2-4 stages; 1: two CTAs per SM, up to 255
+ *                                registers, up to 6 stages) */
 enum bpmax_tuning_key {
     BPMAX_TUNE_R0_PAIRS_PER_JOB = 0,
     BPMAX_TUNE_R0_MERGE_ITEMS = 1,
     BPMAX_TUNE_CLASS_STREAMS = 2,
     BPMAX_TUNE_WAIT_LIMIT_US = 3,
-    BPMAX_TUNE_INJECT_WAIT_TIMEOUT = 4
+    BPMAX_TUNE_INJECT_WAIT_TIMEOUT = 4,
+    BPMAX_TUNE_WIDE_STAGES = 5,
+    BPMAX_TUNE_R0_VARIANT = 6
 };
 int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value);
 int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value);
 
-/* Autotuner: fills the given pairs under each candidate setting of the three tunables (pairs per
- * job 8 / 32 / unbounded, merge cost 1 / 4, class streams on / off when the batch has several
- * width classes), timing `trials` graph replays of each after one capture run, and keeps the
- * fastest setting for these shapes: later fills of the same shapes use it. best (may be NULL)
- * receives the 3 chosen values in key order, best_ms (may be NULL) the fill time in ms. Results of
- * every fill are unchanged by any setting (bit for bit). No reference counterpart. */
+/* Autotuner: fills the given pairs under candidate settings of the schedule tunables, timing
+ * `trials` graph replays of each after one capture run, and keeps the fastest setting for these
+ * shapes: later fills of the same shapes use it. It first tries every combination of pairs per job
+ * (8 / 32 / unbounded), merge cost (1 / 4) and class streams (on / off, when the batch has several
+ * width classes) with the default kernel shapes, then, on the best of those, the other product
+ * kernel shape (BPMAX_TUNE_R0_VARIANT 1, when a strand-2 length is <= 64) and the deeper tile ring
+ * (BPMAX_TUNE_WIDE_STAGES 3, when one is in 65..320). best (may be NULL) receives the 5 chosen values
+ * of keys 0, 1, 2, 6, 5 in that order; best_ms (may be NULL) the fill time in ms. Results of every
+ * fill are unchanged by any setting (bit for bit). The reference's counterpart is choosing its tile
+ * arguments N_tile, MR, NR by hand (V3/bpmax.c:129). */
 int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, const long *Ms,
                        const int *const *seq2s, const long *Ns, int trials, long *best, float *best_ms);
 

@@ -175,16 +175,21 @@ def test_batched_mixed_widths(eng, oracle_mod):
 
 def test_tuning_settings_keep_results(eng, oracle_mod):
     """Every schedule setting changes how the work is cut, never a result bit."""
-    pairs = [W.pair(m, n, 80 + i) for i, (m, n) in enumerate([(23, 61), (17, 30), (9, 12), (31, 64), (6, 45)])]
+    pairs = [W.pair(m, n, 80 + i) for i, (m, n) in enumerate([(23, 61), (17, 30), (9, 12), (31, 64), (6, 45),
+                                                                (7, 150), (5, 250)])]
     eng.set_weights(W.INTEGER_WEIGHTS)
     exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
                    dtype=np.float32)
-    saved = {k: eng.get_tuning(k) for k in ("r0_pairs_per_job", "r0_merge_items", "class_streams")}
+    keys = ("r0_pairs_per_job", "r0_merge_items", "class_streams", "r0_variant", "wide_stages")
+    saved = {k: eng.get_tuning(k) for k in keys}
     try:
-        for ppj, merge, streams in [(1, 0, 1), (3, 16, 0), (1 << 20, 2, 1), (2, 1, 0)]:
+        for ppj, merge, streams, variant, stages in [(1, 0, 1, 0, 2), (3, 16, 0, 1, 3), (1 << 20, 2, 1, 1, 2),
+                                                     (2, 1, 0, 0, 3)]:
             eng.set_tuning("r0_pairs_per_job", ppj)
             eng.set_tuning("r0_merge_items", merge)
             eng.set_tuning("class_streams", streams)
+            eng.set_tuning("r0_variant", variant)
+            eng.set_tuning("wide_stages", stages)
             assert np.array_equal(bits(eng.score_batch(pairs)), bits(exp))
             F, _ = eng.fill_compact(*pairs[0])
             Fo, _, _ = oracle_mod.fill(*pairs[0], W.INTEGER_WEIGHTS)
@@ -196,11 +201,13 @@ def test_tuning_settings_keep_results(eng, oracle_mod):
 
 def test_autotune_picks_a_setting_and_keeps_results(eng, oracle_mod):
     wl = W.batched_uneven(num_pairs=10, seed=79, m_range=(2, 28), n_range=(1, 64))
+    wl.pairs += [W.pair(9, 140, 78), W.pair(6, 200, 77)]  # two tile-image widths
     eng.set_weights(wl.weights)
     before = eng.score_batch(wl.pairs)
     best, ms = eng.autotune(wl.pairs, trials=1)
     assert best["r0_pairs_per_job"] in (8, 32, 1 << 20) and best["r0_merge_items"] in (1, 4)
-    assert best["class_streams"] in (0, 1) and ms > 0
+    assert best["class_streams"] in (0, 1) and best["r0_variant"] in (0, 1) and best["wide_stages"] in (2, 3)
+    assert ms > 0
     after = eng.score_batch(wl.pairs)
     exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, wl.weights)[0], len(a), len(b)) for a, b in wl.pairs],
                    dtype=np.float32)
