@@ -434,46 +434,18 @@ finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob 
                 (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(Fc[wide_pos(NTL, r, c)], s1v + S2[q]);
     }
     __syncthreads();
-    // A warp's work of one step is the sequence of (e2, 32-cell chunk of i2) items; it takes them FB
-    // at a time, issuing the 2 FB S2 loads (L2-resident global memory) before any of the updates,
-    // so that their latencies overlap instead of adding up item by item.
-    constexpr int FB = 4;
     for (int e = 0; e + 1 < N; ++e) {
         const float *De = D + drow(Np, e);
-        int e2 = e + 1 + warp, c = 0;  // next item of this warp
-        while (e2 < N) {
-            float r1[FB], r2[FB];
-            int ie2[FB], ii2[FB];
-#pragma unroll
-            for (int u = 0; u < FB; ++u) {
-                ie2[u] = N;
-                if (e2 < N) {
-                    const int i2 = 32 * c + lane;
-                    const float *S2r = S2D + (long long)(e2 - e - 1) * Np;
-                    ie2[u] = e2;
-                    ii2[u] = i2;
-                    const bool ok = i2 < N - e2;
-                    r1[u] = ok ? S2r[i2 + e + 1] : 0.0f;
-                    r2[u] = ok ? S2r[i2] : 0.0f;
-                    if (32 * (c + 1) < N - e2) {
-                        ++c;
-                    } else {
-                        c = 0;
-                        e2 += WARPS;
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < FB; ++u) {
-                const int f2 = ie2[u], i2 = ii2[u];
-                if (f2 < N && i2 < N - f2) {
-                    const int j2 = i2 + f2;
-                    float *Dw = D + drow(Np, f2);
-                    float v = fmax3(Dw[i2], De[i2] + r1[u], r2[u] + De[j2 - e]);
-                    if (f2 == e + 1 && f2 >= 4)  // SW2 when the cell becomes final
-                        v = fmaxf(v, D[drow(Np, f2 - 2) + i2 + 1] + score_w(wsh, sb[i2], sb[j2]));
-                    Dw[i2] = v;
-                }
+        for (int e2 = e + 1 + warp; e2 < N; e2 += WARPS) {
+            float *Dw = D + drow(Np, e2);
+            const float *S2r = S2D + (long long)(e2 - e - 1) * Np;
+            const bool fin = e2 == e + 1 && e2 >= 4;
+            const float *Dp = D + drow(Np, max(e2 - 2, 0)) + 1;
+            for (int i2 = lane; i2 < N - e2; i2 += 32) {
+                const int j2 = i2 + e2;
+                float v = fmax3(Dw[i2], De[i2] + S2r[i2 + e + 1], S2r[i2] + De[j2 - e]);
+                if (fin) v = fmaxf(v, Dp[i2] + score_w(wsh, sb[i2], sb[j2]));
+                Dw[i2] = v;
             }
         }
         __syncthreads();
