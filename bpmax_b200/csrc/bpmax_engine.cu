@@ -35,8 +35,8 @@ using namespace bpmax;
 namespace {
 
 // schedule tunables in key order: pairs per job, merge cost, class streams, product shape variant,
-// tile-product stages
-using Tuned = std::array<int, 5>;
+// tile-product stages, class shares
+using Tuned = std::array<int, 6>;
 
 constexpr int MAX_SMALL_NP = 64;
 constexpr int MAX_CLASS_STREAMS = 8;  // side streams for the per-width-class chains of a batch
@@ -80,7 +80,8 @@ struct Plan {
     // per diagonal and Np class (index NB-1): ranges in the job arrays
     // np = inner table width class; part (product launches): 0 = reads only diagonals <= d-2,
     // 1 = reads diagonal d-1 too
-    struct Launch { int d, np, first, count, s1_first = 0, s1_count = 0, part = 1; };
+    // cap: at most this many CTAs (0: as many as are resident), from the class shares
+    struct Launch { int d, np, first, count, s1_first = 0, s1_count = 0, part = 1, cap = 0; };
     std::vector<Launch> r0_launches, fin_launches;
     std::vector<R0Job> r0_jobs;
     std::vector<R0JobL> r0l_jobs;  // jobs of launches with np > WIDE_TILE_MAX_NP (first/count index this array)
@@ -88,7 +89,7 @@ struct Plan {
     std::vector<CellJob> cell_jobs;
     std::vector<int> classes;  // distinct inner widths, ascending
     int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
-    int r0_variant = 0, wide_stages = 2;
+    int r0_variant = 0, wide_stages = 2, class_share = 0;
     bool r0_only = false;  // R0-only double max-plus (bpmax_gpu_r0_only) instead of the BPMax fill
     bool split = true;     // the product's offset pair 0 may run as its own launch (one-class plans)
     std::vector<cudaEvent_t> diag_ev;  // one pair only: outer diagonal d finalized (recorded by the graph)
@@ -127,6 +128,7 @@ struct bpmax_ctx {
     int class_streams = 1;                          // run the width classes of a batch on parallel streams
     int r0_variant = 0;                             // shape variant of the width-64 product kernel (0 or 1)
     int wide_stages = 2;                            // shared-memory stages of the tile-image product (2 or 3)
+    int class_share = 0;                            // cap each width class's product CTAs by its share of the work
     // bounded waits of the product kernels: time limit of one wait, and the one-shot test mode in
     // which the next fill's product kernels issue no copies (their first waits run out)
     unsigned long long wait_ns = 4000000000ULL;
@@ -207,6 +209,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     P.split = ctx->allow_split;
     P.r0_variant = ctx->r0_variant;
     P.wide_stages = ctx->wide_stages;
+    P.class_share = ctx->class_share;
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
     if (tu != ctx->tuned.end()) {
         P.pairs_per_job = tu->second[0];
@@ -214,6 +217,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         P.class_streams = tu->second[2];
         P.r0_variant = tu->second[3];
         P.wide_stages = tu->second[4];
+        P.class_share = tu->second[5];
     }
     const int n = (int)Ms.size();
     long long f = 0, s = 0;
@@ -252,6 +256,26 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     std::sort(classes.begin(), classes.end());
     classes.erase(std::unique(classes.begin(), classes.end()), classes.end());
     P.classes = classes;
+    // class shares: with several width classes on parallel graph branches, a product launch of one
+    // class may hold every SM until its last job ends, so the branches run one after another. With
+    // class shares on, each class's product launches take at most its share of the resident CTAs
+    // (its share of the padded product terms, at least 1/16), so every branch keeps progressing.
+    std::map<int, double> share;
+    if (P.class_share && classes.size() > 1 && P.class_streams) {
+        auto C3 = [](double x) { return x * (x * x - 1) / 6; };
+        auto T2 = [](double x) { return x * (x + 1) / 2; };
+        double tot = 0;
+        for (const auto &pd : P.pairs) {
+            const double w = C3(pd.M) * (C3(pd.Np) + 2 * T2(pd.Np));
+            share[pd.Np] += w;
+            tot += w;
+        }
+        for (auto &kv : share) kv.second = std::max(kv.second / tot, 1.0 / 16);
+    }
+    auto capped = [&](int np, long long resident) {
+        const auto it = share.find(np);
+        return it == share.end() ? resident : std::max(1LL, (long long)std::llround(resident * it->second));
+    };
     // jobs, grouped by diagonal then inner width class
     const int target = 4 * ctx->sms;  // CTAs per diagonal launch worth splitting k1 for (wide tables)
     for (int d = 0; d < P.maxM; ++d) {
@@ -273,7 +297,8 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 // offset d-1-w) fall in the same pair chunk
                 const int NB = np / 8, G = R0_TAB_ITEMS[NB];
                 const long long P2 = (d + 1) / 2;  // offset pairs per cell
-                const long long resident = (long long)std::max(1, ctx->r0_occ_v[P.r0_variant][NB]) * ctx->sms;
+                const long long resident =
+                    capped(np, (long long)std::max(1, ctx->r0_occ_v[P.r0_variant][NB]) * ctx->sms);
                 const long long qmin = std::max(1, (G + 1) / 2), qmax = std::max<long long>(P.pairs_per_job, qmin);
                 // Offset pair 0 (offsets 0 and d-1) is the only one that reads diagonal d-1. In a plan
                 // of one width class, where one iteration holds at most 2 items, it becomes its own
@@ -282,6 +307,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 const long long first_pair = (P.split && classes.size() == 1 && G <= 2 && P2 > 1) ? 1 : 0;
                 if (first_pair) {
                     Plan::Launch rb{d, np, (int)P.r0_jobs.size(), 0};
+                    rb.cap = share.empty() ? 0 : (int)resident;
                     for (int p = 0; p < n; ++p)
                         if (P.pairs[p].Np == np && Ms[p] > d)
                             for (int i1 = 0; i1 < Ms[p] - d; ++i1) P.r0_jobs.push_back(R0Job{p, i1, 0, 1});
@@ -291,6 +317,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 const long long q = r0_pairs_per_job(cells, P2 - first_pair, resident, qmin, qmax, P.merge_items);
                 Plan::Launch rl{d, np, (int)P.r0_jobs.size(), 0};
                 rl.part = first_pair ? 0 : 1;
+                rl.cap = share.empty() ? 0 : (int)resident;
                 for (long long c0 = first_pair; c0 < P2; c0 += q)
                     for (int p = 0; p < n; ++p)
                         if (P.pairs[p].Np == np && Ms[p] > d)
@@ -306,7 +333,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 // warp task steps of both of its items, DD 3.3, DA and DB 12, F 16 per item
                 const int NT = np / 64;
                 const long long P2 = (d + 1) / 2;
-                const long long resident = (long long)std::max(1, ctx->wide_occ[P.wide_stages]) * ctx->sms;
+                const long long resident = capped(np, (long long)std::max(1, ctx->wide_occ[P.wide_stages]) * ctx->sms);
                 std::vector<std::pair<double, int>> tiles;  // (cost per offset pair, BI << 8 | BJ)
                 double per_pair = 0;
                 for (int BI = 0; BI < NT; ++BI)
@@ -330,7 +357,9 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
                 // jobs of the same offset pairs together (both uses of a table meet in L2), heavy tiles first
                 std::stable_sort(P.r0w_jobs.begin() + first, P.r0w_jobs.end(),
                                  [](const R0JobW &a, const R0JobW &b) { return a.p0 < b.p0; });
-                P.r0_launches.push_back(Plan::Launch{d, np, (int)first, (int)(P.r0w_jobs.size() - first)});
+                Plan::Launch wl{d, np, (int)first, (int)(P.r0w_jobs.size() - first)};
+                wl.cap = share.empty() ? 0 : (int)resident;
+                P.r0_launches.push_back(wl);
                 continue;
             }
             const int nbk = np / 64;
@@ -370,7 +399,7 @@ void launch_r0_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 template <int STAGES>
 void launch_r0_wide_t(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
-    const int grid = std::min(L.count, std::max(1, ctx->wide_occ[STAGES]) * ctx->sms);
+    const int grid = std::min(L.count, L.cap > 0 ? L.cap : std::max(1, ctx->wide_occ[STAGES]) * ctx->sms);
     r0_wide_kernel<STAGES><<<grid, WideCfg<STAGES>::THREADS, WideCfg<STAGES>::SMEM, s>>>(
         (const R0JobW *)ctx->r0wjobs.p + L.first, L.count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
         wait_ctl(ctx));
@@ -405,7 +434,8 @@ template <int NB, int V>
 void launch_r0_v(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
     using C = R0Cfg<NB, V>;
-    const int grid = std::min(L.count, std::max(1, ctx->r0_occ_v[V][NB]) * ctx->sms);  // resident CTAs; each loops over jobs
+    // resident CTAs (or the class's share of them); each loops over jobs
+    const int grid = std::min(L.count, L.cap > 0 ? L.cap : std::max(1, ctx->r0_occ_v[V][NB]) * ctx->sms);
     r0_kernel<NB, V><<<grid, C::THREADS, C::SMEM, s>>>((const R0Job *)ctx->r0jobs.p + L.first, L.count,
                                                        (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, L.d,
                                                        wait_ctl(ctx));
@@ -660,10 +690,10 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
     const Tuned want = tu != ctx->tuned.end() ? tu->second
                                               : Tuned{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams,
-                                                      ctx->r0_variant, ctx->wide_stages};
+                                                      ctx->r0_variant, ctx->wide_stages, ctx->class_share};
     const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
                              ctx->plan.class_streams == want[2] && ctx->plan.r0_variant == want[3] &&
-                             ctx->plan.wide_stages == want[4];
+                             ctx->plan.wide_stages == want[4] && ctx->plan.class_share == want[5];
     if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only &&
           ctx->plan.split == ctx->allow_split)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
@@ -1233,6 +1263,9 @@ int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value)
         if (value != 0 && value != 1) return fail(ctx, BPMAX_EINVAL, "product shape variant must be 0 or 1");
         ctx->r0_variant = (int)value;
         break;
+    case BPMAX_TUNE_CLASS_SHARE:
+        ctx->class_share = value != 0;
+        break;
     default: return fail(ctx, BPMAX_EINVAL, "unknown tuning key %d", key);
     }
     return BPMAX_OK;
@@ -1249,6 +1282,7 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value)
     case BPMAX_TUNE_INJECT_WAIT_TIMEOUT: *value = ctx->inject_wait_timeout ? 1 : 0; break;
     case BPMAX_TUNE_WIDE_STAGES: *value = ctx->wide_stages; break;
     case BPMAX_TUNE_R0_VARIANT: *value = ctx->r0_variant; break;
+    case BPMAX_TUNE_CLASS_SHARE: *value = ctx->class_share; break;
     default: return BPMAX_EINVAL;
     }
     return BPMAX_OK;
@@ -1266,7 +1300,8 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
     }
     const std::vector<int> key = shape_key(vm, vn);
     ctx->tuned.erase(key);
-    const Tuned saved{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams, ctx->r0_variant, ctx->wide_stages};
+    const Tuned saved{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams,
+                      ctx->r0_variant,       ctx->wide_stages,    ctx->class_share};
     std::set<int> classes;
     bool small = false, tiled = false;
     for (int n : vn) {
@@ -1284,6 +1319,7 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
         ctx->class_streams = c[2];
         ctx->r0_variant = c[3];
         ctx->wide_stages = c[4];
+        ctx->class_share = c[5];
         float t = -1.f;
         for (int r = 0; r < 1 + std::max(1, trials) && st == BPMAX_OK; ++r) {  // first run captures the graph
             st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
@@ -1300,20 +1336,23 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
         if (sc == 0 && classes.size() < 2) continue;  // one class: the stream setting changes nothing
         for (int jc : jobs_cand)
             for (int mc : merge_cand)
-                if (st == BPMAX_OK) try_cfg(Tuned{jc, mc, sc, 0, 2});
+                if (st == BPMAX_OK) try_cfg(Tuned{jc, mc, sc, 0, 2, 0});
     }
+    if (classes.size() > 1 && best_cfg[2] == 1 && st == BPMAX_OK)
+        try_cfg(Tuned{best_cfg[0], best_cfg[1], 1, 0, 2, 1});
     const Tuned sched = best_cfg;
-    if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4]});
-    if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3});
+    if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4], sched[5]});
+    if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3, sched[5]});
     ctx->r0_pairs_per_job = saved[0];
     ctx->r0_merge_items = saved[1];
     ctx->class_streams = saved[2];
     ctx->r0_variant = saved[3];
     ctx->wide_stages = saved[4];
+    ctx->class_share = saved[5];
     if (st != BPMAX_OK) return st;
     ctx->tuned[key] = best_cfg;
     if (best)
-        for (int k = 0; k < 5; ++k) best[k] = best_cfg[k];
+        for (int k = 0; k < 6; ++k) best[k] = best_cfg[k];
     if (best_ms) *best_ms = best_t;
     return BPMAX_OK;
 }

@@ -194,7 +194,7 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
         if (lane == 0) last = atomicAdd(done_cnt + stage, 1) == C::WARPS - 1;
         last = __shfl_sync(0xffffffffu, last, 0);
         if (last) {
-            const bool refill = pj < njobs && !__any_sync(0xffffffffu, bad) && !ctl.inject;
+            const bool refill = pj < njobs && !__any_sync(0xffffffffu, bad);  // (test mode: every warp is bad)
             if (lane == 0) {
                 done_cnt[stage] = 0;
                 if (refill) fill_stage(stage, pj, pit);
@@ -223,9 +223,7 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
                     }
             }
             if (__syncthreads_or(bad)) {  // no thread arms or issues from here on
-                if (tid == 0)
-                    for (int s = 0; s < S; ++s)
-                        if (armed[s] > 0) mbar_wait(smem_u32(bars + s), (unsigned)(armed[s] - 1) & 1u, ctl.wait_ns);
+                if (tid == 0) mbar_drain(bars, armed, S, ctl.wait_ns);
                 return;
             }
             jid += gridDim.x;

@@ -180,16 +180,17 @@ def test_tuning_settings_keep_results(eng, oracle_mod):
     eng.set_weights(W.INTEGER_WEIGHTS)
     exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
                    dtype=np.float32)
-    keys = ("r0_pairs_per_job", "r0_merge_items", "class_streams", "r0_variant", "wide_stages")
+    keys = ("r0_pairs_per_job", "r0_merge_items", "class_streams", "r0_variant", "wide_stages", "class_share")
     saved = {k: eng.get_tuning(k) for k in keys}
     try:
-        for ppj, merge, streams, variant, stages in [(1, 0, 1, 0, 2), (3, 16, 0, 1, 3), (1 << 20, 2, 1, 1, 2),
-                                                     (2, 1, 0, 0, 3)]:
+        for ppj, merge, streams, variant, stages, share in [(1, 0, 1, 0, 2, 1), (3, 16, 0, 1, 3, 0),
+                                                            (1 << 20, 2, 1, 1, 2, 1), (2, 1, 0, 0, 3, 0)]:
             eng.set_tuning("r0_pairs_per_job", ppj)
             eng.set_tuning("r0_merge_items", merge)
             eng.set_tuning("class_streams", streams)
             eng.set_tuning("r0_variant", variant)
             eng.set_tuning("wide_stages", stages)
+            eng.set_tuning("class_share", share)
             assert np.array_equal(bits(eng.score_batch(pairs)), bits(exp))
             F, _ = eng.fill_compact(*pairs[0])
             Fo, _, _ = oracle_mod.fill(*pairs[0], W.INTEGER_WEIGHTS)
@@ -207,6 +208,7 @@ def test_autotune_picks_a_setting_and_keeps_results(eng, oracle_mod):
     best, ms = eng.autotune(wl.pairs, trials=1)
     assert best["r0_pairs_per_job"] in (8, 32, 1 << 20) and best["r0_merge_items"] in (1, 4)
     assert best["class_streams"] in (0, 1) and best["r0_variant"] in (0, 1) and best["wide_stages"] in (2, 3)
+    assert best["class_share"] in (0, 1)
     assert ms > 0
     after = eng.score_batch(wl.pairs)
     exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, wl.weights)[0], len(a), len(b)) for a, b in wl.pairs],
