@@ -493,9 +493,34 @@ void launch_r0only_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     }
 }
 
+// Every kernel of a fill prefers the largest shared-memory carveout. An SM runs CTAs of different
+// kernels side by side only when they use the same L1 / shared-memory split; with the driver's
+// per-kernel choice, the product and finalize launches of different width classes (parallel
+// branches of a batch's graph) and the split product launches of one class could not share SMs.
+template <typename K>
+int prefer_smem(bpmax_ctx *ctx, K kernel)
+{
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    return BPMAX_OK;
+}
+
 template <int NB>
 int set_smem_attr(bpmax_ctx *ctx)
 {
+    int st;
+    if ((st = prefer_smem(ctx, r0_kernel<NB>)) || (st = prefer_smem(ctx, r0_kernel<NB, 1>)) ||
+        (st = prefer_smem(ctx, finalize_small_kernel<8 * NB>)) || (st = prefer_smem(ctx, r0only_finalize_small_kernel<8 * NB>)))
+        return st;
+    if constexpr (8 * NB >= 48)
+        if ((st = prefer_smem(ctx, finalize_small_kernel<8 * NB, FIN_BULK_THREADS>))) return st;
+    if (NB == 8)
+        if ((st = prefer_smem(ctx, r0_wide_kernel<2>)) || (st = prefer_smem(ctx, r0_wide_kernel<3>)) ||
+            (st = prefer_smem(ctx, r0_large_kernel)) || (st = prefer_smem(ctx, finalize_wide_kernel)) ||
+            (st = prefer_smem(ctx, finalize_large_kernel)) || (st = prefer_smem(ctx, single_strand_kernel)) ||
+            (st = prefer_smem(ctx, s2_aux_kernel)) || (st = prefer_smem(ctx, r0only_finalize_tile_kernel)) ||
+            (st = prefer_smem(ctx, r0only_finalize_wide_kernel)) || (st = prefer_smem(ctx, r0only_prep_kernel)) ||
+            (st = prefer_smem(ctx, gather_scores_kernel)))
+            return st;
     CK(cudaFuncSetAttribute(r0_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM));
     CK(cudaFuncSetAttribute(r0_kernel<NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB, 1>::SMEM));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ_v[1][NB], r0_kernel<NB, 1>, R0Cfg<NB, 1>::THREADS,

@@ -128,10 +128,10 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
     unsigned phase = 0;
     int stage = 0;
     bool bad = false;  // as in r0_kernel: a wait ran out; no more copies, leave at the next job end
+    int tile = jobs[jid].tile, kbi = 0;  // the job's output tile; k tile of the item = BI + kbi
 #pragma unroll 1
     while (true) {
-        const int tile = jobs[jid].tile;
-        const int BI = tile >> 8, BJ = tile & 0xff, KB = BI + it % (BJ - BI + 1);
+        const int BI = tile >> 8, BJ = tile & 0xff, KB = BI + kbi;
         if (!bad && !mbar_wait(smem_u32(bars + stage), (phase >> stage) & 1u, ctl.wait_ns)) {
             atomicExch(ctl.err, 1);
             bad = true;
@@ -201,6 +201,7 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
             }
         }
         if (pj < njobs) advance(pj, pitems, pit);
+        if (++kbi > BJ - BI) kbi = 0;
         if (++it >= items) {  // job done: merge the partial maxima into the output tile
             const R0JobW job = jobs[jid];
             const PairDesc pd = pairs[job.pair];
@@ -228,8 +229,11 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
             }
             jid += gridDim.x;
             if (jid >= njobs) break;
-            items = job_items(jobs[jid]);
+            const R0JobW nx = jobs[jid];
+            items = job_items(nx);
+            tile = nx.tile;
             it = 0;
+            kbi = 0;
         }
         stage = (stage + 1) % S;
     }

@@ -222,4 +222,4 @@ def test_tuning_rejects_bad_values(eng):
     with pytest.raises(BpmaxError):
         eng.set_tuning("r0_pairs_per_job", 0)
     with pytest.raises(BpmaxError):
-        eng._check(eng._L.bpmax_gpu_set_tuning(eng._ctx, 7, 1))
+        eng._check(eng._L.bpmax_gpu_set_tuning(eng._ctx, 99, 1))
