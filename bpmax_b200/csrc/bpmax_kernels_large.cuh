@@ -434,13 +434,9 @@ finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob 
                 (d == 0 && r == c) ? score_w(wsh + 6, s1[i1], sb[r]) : fmaxf(Fc[wide_pos(NTL, r, c)], s1v + S2[q]);
     }
     __syncthreads();
-    // warp w takes the open diagonals at positions w and 63-w of every 64 (long with short), so the
-    // warps reach the step's barrier with about the same work
     for (int e = 0; e + 1 < N; ++e) {
         const float *De = D + drow(Np, e);
-        for (int q = 0; q < 2 * ((N - 1 - e + 63) / 64); ++q) {
-            const int e2 = e + 1 + 64 * (q >> 1) + ((q & 1) ? 2 * WARPS - 1 - warp : warp);
-            if (e2 >= N) continue;
+        for (int e2 = e + 1 + warp; e2 < N; e2 += WARPS) {
             float *Dw = D + drow(Np, e2);
             const float *S2r = S2D + (long long)(e2 - e - 1) * Np;
             const bool fin = e2 == e + 1 && e2 >= 4;
