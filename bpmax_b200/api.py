@@ -220,9 +220,11 @@ class Engine:
         return out
 
     TUNING_KEYS = {"r0_pairs_per_job": 0, "r0_merge_items": 1, "class_streams": 2, "wait_limit_us": 3,
-                   "inject_wait_timeout": 4, "wide_stages": 5, "r0_variant": 6, "class_share": 7}
+                   "inject_wait_timeout": 4, "wide_stages": 5, "r0_variant": 6, "class_share": 7,
+                   "persistent": 8}
     #: the tunables bpmax_gpu_autotune chooses, in the order it reports them
-    AUTOTUNED = ("r0_pairs_per_job", "r0_merge_items", "class_streams", "r0_variant", "wide_stages", "class_share")
+    AUTOTUNED = ("r0_pairs_per_job", "r0_merge_items", "class_streams", "r0_variant", "wide_stages", "class_share",
+                 "persistent")
 
     def set_tuning(self, key: str, value: int) -> None:
         self._check(self._L.bpmax_gpu_set_tuning(self._ctx, self.TUNING_KEYS[key], int(value)))

@@ -16,7 +16,7 @@ LIB = os.path.join(HERE, "libbpmax_gpu.so")
 
 SOURCES = ["bpmax_engine.cu", "bpmax_shim.cpp"]
 HEADERS = ["bpmax_kernels.cuh", "bpmax_kernels_large.cuh", "bpmax_r0.cuh", "bpmax_adjoint.cuh", "bpmax_r0only.cuh",
-           "bpmax_wide.cuh", "r0_tables.inc", "wide_tables.inc"]
+           "bpmax_wide.cuh", "bpmax_persist.cuh", "r0_tables.inc", "wide_tables.inc"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

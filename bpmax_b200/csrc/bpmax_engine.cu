@@ -29,14 +29,15 @@
 #include "bpmax_adjoint.cuh"
 #include "bpmax_r0only.cuh"
 #include "bpmax_wide.cuh"
+#include "bpmax_persist.cuh"
 
 using namespace bpmax;
 
 namespace {
 
 // schedule tunables in key order: pairs per job, merge cost, class streams, product shape variant,
-// tile-product stages, class shares
-using Tuned = std::array<int, 6>;
+// tile-product stages, class shares, persistent fill
+using Tuned = std::array<int, 7>;
 
 constexpr int MAX_SMALL_NP = 64;
 constexpr int MAX_CLASS_STREAMS = 8;  // side streams for the per-width-class chains of a batch
@@ -89,10 +90,18 @@ struct Plan {
     std::vector<CellJob> cell_jobs;
     std::vector<int> classes;  // distinct inner widths, ascending
     int pairs_per_job = 0, merge_items = 0, class_streams = 1;  // tunables the plan was built with
-    int r0_variant = 0, wide_stages = 2, class_share = 0;
+    int r0_variant = 0, wide_stages = 2, class_share = 0, persist = 0;
     bool r0_only = false;  // R0-only double max-plus (bpmax_gpu_r0_only) instead of the BPMax fill
     bool split = true;     // the product's offset pair 0 may run as its own launch (one-class plans)
     std::vector<cudaEvent_t> diag_ev;  // one pair only: outer diagonal d finalized (recorded by the graph)
+    // persistent fill (one launch per width class walking the diagonals with dependency counters):
+    // the work queues of all classes back to back, each class's range and CTA count
+    bool persistent = false, copyout = false;
+    std::vector<PItem> pitems;
+    struct PClass { int np, first, count, ctas; };
+    std::vector<PClass> pclasses;
+    std::vector<int> prod_need;  // per cell (PairDesc::cell_base + cell): product jobs
+    int n_counters = 0;          // per-diagonal counters of all pairs
     cudaGraphExec_t graph = nullptr;
     long launches = 0;
 };
@@ -115,6 +124,8 @@ struct bpmax_ctx {
     std::string err;
     DevBuf F, FT, S, bases, pairs, r0jobs, r0ljobs, r0wjobs, celljobs, scores, conv, tbstack, grads, tbstatus, errflag;
     DevBuf r0vals;         // R0-only mode: seq1 then seq2 of the pair, as floats
+    DevBuf pq, pcnt, pneed;  // persistent fill: work queue; counters (class heads, diagonals, cells); jobs per cell
+    bool copyout = false;    // the next fill copies the reference layout out per diagonal (graph path)
     bool r0_only = false;  // mode of the next prepare()
     // schedule of the next prepare(): with the reference-layout copy-out running beside the fill
     // (bpmax_gpu_fill), the unsplit product leaves the SMs the row conversions need
@@ -129,6 +140,8 @@ struct bpmax_ctx {
     int r0_variant = 0;                             // shape variant of the width-64 product kernel (0 or 1)
     int wide_stages = 2;                            // shared-memory stages of the tile-image product (2 or 3)
     int class_share = 0;                            // cap each width class's product CTAs by its share of the work
+    int persist = 0;                                // fill width classes <= 64 with the persistent kernel
+    int persist_occ[9] = {};                        // resident persistent-fill CTAs per SM, per width class
     // bounded waits of the product kernels: time limit of one wait, and the one-shot test mode in
     // which the next fill's product kernels issue no copies (their first waits run out)
     unsigned long long wait_ns = 4000000000ULL;
@@ -198,6 +211,74 @@ std::vector<int> shape_key(const std::vector<int> &Ms, const std::vector<int> &N
     return k;
 }
 
+// Work queue of the persistent fill, per width class: for d = 1, 2, ... the product jobs of
+// diagonal d with offset pairs >= 1, then the finalize items of diagonal d-1, then the jobs of d for
+// offset pair 0 (the only ones reading diagonal d-1); the finalize items of the last diagonal close
+// it. Every item depends only on items before it (bpmax_persist.cuh). Jobs of one group are ordered
+// by pair chunk, then cell, as in the graph path. A class's CTA count is its share of the resident
+// CTAs when several classes run side by side (its share of the padded product terms).
+void build_queue(bpmax_ctx *ctx, Plan &P)
+{
+    const int n = (int)P.pairs.size();
+    long long ncells = 0;
+    for (const auto &pd : P.pairs) ncells += (long long)pd.M * (pd.M + 1) / 2;
+    P.prod_need.assign(ncells, 0);
+    P.pitems.clear();
+    P.pclasses.clear();
+    auto C3 = [](double x) { return x * (x * x - 1) / 6; };
+    auto T2 = [](double x) { return x * (x + 1) / 2; };
+    std::map<int, double> work;
+    double tot = 0;
+    for (const auto &pd : P.pairs) {
+        const double w = C3(pd.M) * (C3(pd.Np) + 2 * T2(pd.Np)) + 1.0;
+        work[pd.Np] += w;
+        tot += w;
+    }
+    for (int np : P.classes) {
+        const int NB = np / 8, G = R0_TAB_ITEMS[NB];
+        const long long full = (long long)std::max(1, ctx->persist_occ[NB]) * ctx->sms;
+        const int ctas = P.classes.size() == 1
+                             ? (int)full
+                             : (int)std::max<long long>(ctx->sms / 8, std::llround(full * work[np] / tot));
+        const int first = (int)P.pitems.size();
+        int maxM = 0;
+        for (const auto &pd : P.pairs)
+            if (pd.Np == np) maxM = std::max(maxM, pd.M);
+        auto fin_items = [&](int e) {
+            for (int p = 0; p < n; ++p)
+                if (P.pairs[p].Np == np && P.pairs[p].M > e)
+                    for (int i1 = 0; i1 < P.pairs[p].M - e; ++i1) P.pitems.push_back(PItem{p, i1, e, 0, 0, 1});
+        };
+        const long long qmin = std::max(1, (G + 1) / 2);
+        for (int d = 1; d <= maxM; ++d) {
+            const long long P2 = (d + 1) / 2;
+            long long cells = 0;
+            for (const auto &pd : P.pairs)
+                if (pd.Np == np && pd.M > d) cells += pd.M - d;
+            if (cells > 0 && P2 > 1) {  // offset pairs >= 1
+                const long long q = r0_pairs_per_job(cells, P2 - 1, ctas, qmin, std::max<long long>(P.pairs_per_job, qmin),
+                                                     P.merge_items);
+                for (long long c0 = 1; c0 < P2; c0 += q)
+                    for (int p = 0; p < n; ++p)
+                        if (P.pairs[p].Np == np && P.pairs[p].M > d)
+                            for (int i1 = 0; i1 < P.pairs[p].M - d; ++i1) {
+                                P.pitems.push_back(PItem{p, i1, d, (int)c0, (int)std::min(c0 + q, P2), 0});
+                                P.prod_need[P.pairs[p].cell_base + cell_index(P.pairs[p].M, i1, i1 + d)] += 1;
+                            }
+            }
+            fin_items(d - 1);
+            if (cells > 0)  // offset pair 0 (offsets 0 and d-1)
+                for (int p = 0; p < n; ++p)
+                    if (P.pairs[p].Np == np && P.pairs[p].M > d)
+                        for (int i1 = 0; i1 < P.pairs[p].M - d; ++i1) {
+                            P.pitems.push_back(PItem{p, i1, d, 0, 1, 0});
+                            P.prod_need[P.pairs[p].cell_base + cell_index(P.pairs[p].M, i1, i1 + d)] += 1;
+                        }
+        }
+        P.pclasses.push_back(Plan::PClass{np, first, (int)P.pitems.size() - first, ctas});
+    }
+}
+
 int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &Ns, Plan &P)
 {
     P = Plan();
@@ -210,6 +291,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     P.r0_variant = ctx->r0_variant;
     P.wide_stages = ctx->wide_stages;
     P.class_share = ctx->class_share;
+    P.persist = ctx->persist;
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
     if (tu != ctx->tuned.end()) {
         P.pairs_per_job = tu->second[0];
@@ -218,6 +300,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         P.r0_variant = tu->second[3];
         P.wide_stages = tu->second[4];
         P.class_share = tu->second[5];
+        P.persist = tu->second[6];
     }
     const int n = (int)Ms.size();
     long long f = 0, s = 0;
@@ -245,6 +328,9 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         b += Ms[p];
         pd.seq2_off = b;
         b += Ns[p];
+        pd.cnt_off = P.n_counters;
+        P.n_counters += Ms[p];
+        pd.cell_base = p == 0 ? 0 : P.pairs.back().cell_base + (long long)P.pairs.back().M * (P.pairs.back().M + 1) / 2;
         P.pairs.push_back(pd);
         P.maxM = std::max(P.maxM, Ms[p]);
     }
@@ -385,6 +471,11 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
     for (auto &fl : P.fin_launches)
         for (const auto &nx : P.fin_launches)
             if (nx.d == fl.d + 1 && nx.np == fl.np) { fl.s1_first = nx.first; fl.s1_count = nx.count; }
+    // the persistent fill: width classes <= 64 only, not the R0-only mode, not the reference-layout
+    // fill with its per-diagonal copy-out (both keep the graph of per-diagonal launches)
+    P.copyout = ctx->copyout;
+    P.persistent = P.persist && !ctx->r0_only && !ctx->copyout && P.classes.back() <= MAX_SMALL_NP;
+    if (P.persistent) build_queue(ctx, P);
     return BPMAX_OK;
 }
 
@@ -442,6 +533,14 @@ void launch_r0_v(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 }
 
 template <int NB>
+void launch_persist(bpmax_ctx *ctx, const PersistCtl &pc, int ctas, cudaStream_t s)
+{
+    fill_persistent_kernel<NB><<<ctas, R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM, s>>>(
+        pc, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W,
+        wait_ctl(ctx));
+}
+
+template <int NB>
 void launch_r0(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaStream_t s)
 {
     if (P.r0_variant == 1)
@@ -493,10 +592,10 @@ void launch_r0only_fin(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     }
 }
 
-// Every kernel of a fill prefers the largest shared-memory carveout. An SM runs CTAs of different
-// kernels side by side only when they use the same L1 / shared-memory split; with the driver's
-// per-kernel choice, the product and finalize launches of different width classes (parallel
-// branches of a batch's graph) and the split product launches of one class could not share SMs.
+// The product kernels, the small finalize and the persistent fill prefer the largest shared-memory
+// carveout: an SM runs CTAs of different kernels side by side only when they use the same L1 /
+// shared-memory split (parallel graph branches of a batch, the persistent launches of its width
+// classes, the split product launches of one class).
 template <typename K>
 int prefer_smem(bpmax_ctx *ctx, K kernel)
 {
@@ -515,12 +614,10 @@ int set_smem_attr(bpmax_ctx *ctx)
         if ((st = prefer_smem(ctx, finalize_small_kernel<8 * NB, FIN_BULK_THREADS>))) return st;
     if (NB == 8)
         if ((st = prefer_smem(ctx, r0_wide_kernel<2>)) || (st = prefer_smem(ctx, r0_wide_kernel<3>)) ||
-            (st = prefer_smem(ctx, r0_large_kernel)) || (st = prefer_smem(ctx, finalize_wide_kernel)) ||
-            (st = prefer_smem(ctx, finalize_large_kernel)) || (st = prefer_smem(ctx, single_strand_kernel)) ||
-            (st = prefer_smem(ctx, s2_aux_kernel)) || (st = prefer_smem(ctx, r0only_finalize_tile_kernel)) ||
-            (st = prefer_smem(ctx, r0only_finalize_wide_kernel)) || (st = prefer_smem(ctx, r0only_prep_kernel)) ||
-            (st = prefer_smem(ctx, gather_scores_kernel)))
+            (st = prefer_smem(ctx, r0_large_kernel)))
             return st;
+    // (the wide finalize kernels keep the driver's choice: their S2 reads live on the L1 that a
+    // larger shared-memory carveout would take away, 389 vs 324 ms at 256x256)
     CK(cudaFuncSetAttribute(r0_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM));
     CK(cudaFuncSetAttribute(r0_kernel<NB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB, 1>::SMEM));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ_v[1][NB], r0_kernel<NB, 1>, R0Cfg<NB, 1>::THREADS,
@@ -532,6 +629,10 @@ int set_smem_attr(bpmax_ctx *ctx)
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FinShape<8 * NB, FIN_BULK_THREADS>::SMEM));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->r0_occ_v[0][NB], r0_kernel<NB>, R0Cfg<NB>::THREADS,
                                                      R0Cfg<NB>::SMEM));
+    CK(cudaFuncSetAttribute(fill_persistent_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)R0Cfg<NB>::SMEM));
+    CK(cudaFuncSetAttribute(fill_persistent_kernel<NB>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->persist_occ[NB], fill_persistent_kernel<NB>,
+                                                     R0Cfg<NB>::THREADS, R0Cfg<NB>::SMEM));
     if (NB == 8) {
         CK(cudaFuncSetAttribute(r0_wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideCfg<2>::SMEM));
         CK(cudaFuncSetAttribute(r0_wide_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideCfg<3>::SMEM));
@@ -590,10 +691,47 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         s2_aux_kernel<<<(int)P.pairs.size(), 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (float *)ctx->S.p);
         launches += 2;
     }
+    const bool prof = kp && kp->on;
+    if (P.persistent) {  // one persistent launch per width class, side by side on the class streams
+        const int nclass = (int)P.pclasses.size();
+        int *cnt = (int *)ctx->pcnt.p;
+        int *diag_done = cnt + 64, *prod_done = diag_done + align64(P.n_counters);
+        CK(cudaMemsetAsync(cnt, 0, ((size_t)64 + align64(P.n_counters) + P.prod_need.size()) * sizeof(int), ctx->stream));
+        const bool pfork = !prof && nclass > 1;
+        if (pfork) {
+            CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
+            for (int k = 0; k < std::min(nclass, MAX_CLASS_STREAMS); ++k)
+                CK(cudaStreamWaitEvent(ctx->class_stream[k], ctx->fork_ev, 0));
+        }
+        for (int c = 0; c < nclass; ++c, ++launches) {
+            const auto &pcl = P.pclasses[c];
+            const cudaStream_t st = pfork ? ctx->class_stream[c % MAX_CLASS_STREAMS] : ctx->stream;
+            const PersistCtl pctl{(const PItem *)ctx->pq.p + pcl.first, pcl.count, cnt + c, diag_done, prod_done,
+                                  (const int *)ctx->pneed.p};
+            ProfScope ps(ctx, kp, 1);
+            switch (pcl.np / 8) {
+            case 1: launch_persist<1>(ctx, pctl, pcl.ctas, st); break;
+            case 2: launch_persist<2>(ctx, pctl, pcl.ctas, st); break;
+            case 3: launch_persist<3>(ctx, pctl, pcl.ctas, st); break;
+            case 4: launch_persist<4>(ctx, pctl, pcl.ctas, st); break;
+            case 5: launch_persist<5>(ctx, pctl, pcl.ctas, st); break;
+            case 6: launch_persist<6>(ctx, pctl, pcl.ctas, st); break;
+            case 7: launch_persist<7>(ctx, pctl, pcl.ctas, st); break;
+            default: launch_persist<8>(ctx, pctl, pcl.ctas, st); break;
+            }
+        }
+        if (pfork)
+            for (int k = 0; k < std::min(nclass, MAX_CLASS_STREAMS); ++k) {
+                CK(cudaEventRecord(ctx->join_ev[k], ctx->class_stream[k]));
+                CK(cudaStreamWaitEvent(ctx->stream, ctx->join_ev[k], 0));
+            }
+        CK(cudaGetLastError());
+        P.launches = launches;
+        return BPMAX_OK;
+    }
     // pairs of different inner widths never interact: each width class runs its own chain of
     // diagonals on its own stream (parallel branches of the captured graph); profiling runs
     // serialise everything on the main stream so every launch can be timed
-    const bool prof = kp && kp->on;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(ctx->stream, &cap));
     const bool capturing = cap == cudaStreamCaptureStatusActive;
@@ -715,10 +853,11 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
     const auto tu = ctx->tuned.find(shape_key(Ms, Ns));
     const Tuned want = tu != ctx->tuned.end() ? tu->second
                                               : Tuned{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams,
-                                                      ctx->r0_variant, ctx->wide_stages, ctx->class_share};
+                                                      ctx->r0_variant, ctx->wide_stages, ctx->class_share, ctx->persist};
     const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
                              ctx->plan.class_streams == want[2] && ctx->plan.r0_variant == want[3] &&
-                             ctx->plan.wide_stages == want[4] && ctx->plan.class_share == want[5];
+                             ctx->plan.wide_stages == want[4] && ctx->plan.class_share == want[5] &&
+                             ctx->plan.persist == want[6] && ctx->plan.copyout == ctx->copyout;
     if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only &&
           ctx->plan.split == ctx->allow_split)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
@@ -742,6 +881,16 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
         if ((st = ensure(ctx, ctx->r0jobs, P.r0_jobs.size() * sizeof(R0Job))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->r0ljobs, P.r0l_jobs.size() * sizeof(R0JobL))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->r0wjobs, P.r0w_jobs.size() * sizeof(R0JobW))) != BPMAX_OK) return st;
+        if (P.persistent) {
+            if ((st = ensure(ctx, ctx->pq, P.pitems.size() * sizeof(PItem))) != BPMAX_OK) return st;
+            if ((st = ensure(ctx, ctx->pneed, P.prod_need.size() * sizeof(int))) != BPMAX_OK) return st;
+            if ((st = ensure(ctx, ctx->pcnt, (64 + align64(P.n_counters) + P.prod_need.size()) * sizeof(int))) != BPMAX_OK)
+                return st;
+            CK(cudaMemcpyAsync(ctx->pq.p, P.pitems.data(), P.pitems.size() * sizeof(PItem), cudaMemcpyHostToDevice,
+                               ctx->stream));
+            CK(cudaMemcpyAsync(ctx->pneed.p, P.prod_need.data(), P.prod_need.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, ctx->stream));
+        }
         if ((st = ensure(ctx, ctx->celljobs, P.cell_jobs.size() * sizeof(CellJob))) != BPMAX_OK) return st;
         if ((st = ensure(ctx, ctx->scores, P.pairs.size() * sizeof(float))) != BPMAX_OK) return st;
         CK(cudaMemcpyAsync(ctx->pairs.p, P.pairs.data(), P.pairs.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, ctx->stream));
@@ -975,7 +1124,8 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
     for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs,
-                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->r0wjobs, &ctx->celljobs, &ctx->scores, &ctx->conv, &ctx->errflag,
+                      &ctx->r0jobs, &ctx->r0ljobs, &ctx->r0wjobs, &ctx->pq, &ctx->pcnt, &ctx->pneed, &ctx->celljobs,
+                      &ctx->scores, &ctx->conv, &ctx->errflag,
                       &ctx->r0vals})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
@@ -1123,8 +1273,10 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
     const bool pinned = is_pinned(F_lin);
     if (!pinned && (st = ensure_host_stage(ctx, row_max * sizeof(float))) != BPMAX_OK) return st;
     ctx->allow_split = false;
+    ctx->copyout = true;
     st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N, true);
     ctx->allow_split = true;
+    ctx->copyout = false;
     if (st != BPMAX_OK) return st;
     const std::vector<cudaEvent_t> &dev = ctx->plan.diag_ev;
     std::vector<long long> pending_n(2, 0);
@@ -1291,6 +1443,9 @@ int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value)
     case BPMAX_TUNE_CLASS_SHARE:
         ctx->class_share = value != 0;
         break;
+    case BPMAX_TUNE_PERSISTENT:
+        ctx->persist = value != 0;
+        break;
     default: return fail(ctx, BPMAX_EINVAL, "unknown tuning key %d", key);
     }
     return BPMAX_OK;
@@ -1308,6 +1463,7 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value)
     case BPMAX_TUNE_WIDE_STAGES: *value = ctx->wide_stages; break;
     case BPMAX_TUNE_R0_VARIANT: *value = ctx->r0_variant; break;
     case BPMAX_TUNE_CLASS_SHARE: *value = ctx->class_share; break;
+    case BPMAX_TUNE_PERSISTENT: *value = ctx->persist; break;
     default: return BPMAX_EINVAL;
     }
     return BPMAX_OK;
@@ -1325,8 +1481,8 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
     }
     const std::vector<int> key = shape_key(vm, vn);
     ctx->tuned.erase(key);
-    const Tuned saved{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams,
-                      ctx->r0_variant,       ctx->wide_stages,    ctx->class_share};
+    const Tuned saved{ctx->r0_pairs_per_job, ctx->r0_merge_items, ctx->class_streams, ctx->r0_variant,
+                      ctx->wide_stages,      ctx->class_share,    ctx->persist};
     std::set<int> classes;
     bool small = false, tiled = false;
     for (int n : vn) {
@@ -1345,6 +1501,7 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
         ctx->r0_variant = c[3];
         ctx->wide_stages = c[4];
         ctx->class_share = c[5];
+        ctx->persist = c[6];
         float t = -1.f;
         for (int r = 0; r < 1 + std::max(1, trials) && st == BPMAX_OK; ++r) {  // first run captures the graph
             st = fill_pairs(ctx, num_pairs, seq1s, Ms, seq2s, Ns);
@@ -1361,23 +1518,27 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
         if (sc == 0 && classes.size() < 2) continue;  // one class: the stream setting changes nothing
         for (int jc : jobs_cand)
             for (int mc : merge_cand)
-                if (st == BPMAX_OK) try_cfg(Tuned{jc, mc, sc, 0, 2, 0});
+                if (st == BPMAX_OK) try_cfg(Tuned{jc, mc, sc, 0, 2, 0, 0});
     }
     if (classes.size() > 1 && best_cfg[2] == 1 && st == BPMAX_OK)
-        try_cfg(Tuned{best_cfg[0], best_cfg[1], 1, 0, 2, 1});
+        try_cfg(Tuned{best_cfg[0], best_cfg[1], 1, 0, 2, 1, 0});
     const Tuned sched = best_cfg;
-    if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4], sched[5]});
-    if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3, sched[5]});
+    if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4], sched[5], 0});
+    if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3, sched[5], 0});
+    if (!tiled && st == BPMAX_OK)  // the persistent fill, with the best pairs per job and merge cost
+        for (int jc : jobs_cand)
+            if (st == BPMAX_OK) try_cfg(Tuned{jc, sched[1], sched[2], 0, sched[4], 0, 1});
     ctx->r0_pairs_per_job = saved[0];
     ctx->r0_merge_items = saved[1];
     ctx->class_streams = saved[2];
     ctx->r0_variant = saved[3];
     ctx->wide_stages = saved[4];
     ctx->class_share = saved[5];
+    ctx->persist = saved[6];
     if (st != BPMAX_OK) return st;
     ctx->tuned[key] = best_cfg;
     if (best)
-        for (int k = 0; k < 6; ++k) best[k] = best_cfg[k];
+        for (int k = 0; k < 7; ++k) best[k] = best_cfg[k];
     if (best_ms) *best_ms = best_t;
     return BPMAX_OK;
 }

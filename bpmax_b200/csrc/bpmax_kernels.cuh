@@ -46,7 +46,8 @@ struct Weights {
 };
 
 struct PairDesc {
-    int M, N, Np, pad0;
+    int M, N, Np;
+    int cnt_off;       // persistent fill: offset of the pair's per-diagonal counters (M ints)
     long long F_off;   // float offset of F[0] (and of FT[0] in the FT arena)
     long long S1_off;  // float offset of S1 in the S arena
     long long S2_off;  // float offset of S2 in the S arena
@@ -55,6 +56,7 @@ struct PairDesc {
     long long S2d_off; // Np > 64 only: S2 diagonal-major, S2D[e][i] = S2(i, i+e), -inf outside
     int seq1_off;      // offset of seq1 in the base arena (uint8)
     int seq2_off;      // offset of the REVERSED seq2 in the base arena (uint8)
+    long long cell_base;  // persistent fill: index of the pair's cell (0, 0) among all pairs' cells
 };
 
 // pair type of ordered bases (a,b): AU=0 UA=1 GC=2 CG=3 GU=4 UG=5, else -1
