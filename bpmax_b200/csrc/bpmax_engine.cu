@@ -140,7 +140,7 @@ struct bpmax_ctx {
     int r0_variant = 0;                             // shape variant of the width-64 product kernel (0 or 1)
     int wide_stages = 2;                            // shared-memory stages of the tile-image product (2 or 3)
     int class_share = 0;                            // cap each width class's product CTAs by its share of the work
-    int persist = 0;                                // fill width classes <= 64 with the persistent kernel
+    int persist = 0;  // width classes <= 64 by the persistent kernel: 0 no, 1 side by side, 2 one after another
     int persist_occ[9] = {};                        // resident persistent-fill CTAs per SM, per width class
     // bounded waits of the product kernels: time limit of one wait, and the one-shot test mode in
     // which the next fill's product kernels issue no copies (their first waits run out)
@@ -211,12 +211,14 @@ std::vector<int> shape_key(const std::vector<int> &Ms, const std::vector<int> &N
     return k;
 }
 
-// Work queue of the persistent fill, per width class: for d = 1, 2, ... the product jobs of
-// diagonal d with offset pairs >= 1, then the finalize items of diagonal d-1, then the jobs of d for
+// Work queue of the persistent fill, per width class: for d = 1, 2, ... the finalize items of
+// diagonal d-1, then the product jobs of diagonal d with offset pairs >= 1, then the jobs of d for
 // offset pair 0 (the only ones reading diagonal d-1); the finalize items of the last diagonal close
-// it. Every item depends only on items before it (bpmax_persist.cuh). Jobs of one group are ordered
-// by pair chunk, then cell, as in the graph path. A class's CTA count is its share of the resident
-// CTAs when several classes run side by side (its share of the padded product terms).
+// it. Every item depends only on items before it (bpmax_persist.cuh), and the finalize of d-1 runs
+// beside the long product group of d. Jobs of one group are ordered by pair chunk, then cell, as in
+// the graph path. CTA counts: one class takes every resident CTA. Several classes either run one
+// after another, each with every resident CTA (mode 2), or side by side (mode 1), each with a number
+// of SMs proportional to its estimated time, so that all of them are resident at once.
 void build_queue(bpmax_ctx *ctx, Plan &P)
 {
     const int n = (int)P.pairs.size();
@@ -225,21 +227,43 @@ void build_queue(bpmax_ctx *ctx, Plan &P)
     P.prod_need.assign(ncells, 0);
     P.pitems.clear();
     P.pclasses.clear();
+    // estimated CTA-microseconds per class: product items (one C(Np)+2T(Np) block each) and
+    // finalizes, at the per-CTA costs of each width measured with this kernel on a B200, per SM
+    // (divided by the CTAs one SM holds)
+    static const double ITEM_US[9] = {0, 0.19, 0.30, 0.42, 0.65, 0.93, 1.2, 2.1, 2.1};
+    static const double FIN_US[9] = {0, 4.0, 6.0, 9.0, 14.0, 24.0, 36.0, 72.0, 80.0};
     auto C3 = [](double x) { return x * (x * x - 1) / 6; };
     auto T2 = [](double x) { return x * (x + 1) / 2; };
-    std::map<int, double> work;
-    double tot = 0;
+    std::map<int, double> sm_time;
+    double sm_tot = 0;
     for (const auto &pd : P.pairs) {
-        const double w = C3(pd.M) * (C3(pd.Np) + 2 * T2(pd.Np)) + 1.0;
-        work[pd.Np] += w;
-        tot += w;
+        const int NB = pd.Np / 8;
+        const double t = (C3(pd.M) * ITEM_US[NB] + T2(pd.M) * FIN_US[NB]) / std::max(1, ctx->persist_occ[NB]);
+        sm_time[pd.Np] += t;
+        sm_tot += t;
+    }
+    std::map<int, int> sms_of;
+    const bool side = P.classes.size() > 1 && P.persist == 1;
+    if (side) {  // SMs per class, all classes resident at once (a margin of 2 SMs for uneven packing)
+        const int budget = std::max((int)P.classes.size(), ctx->sms - 2);
+        int used = 0;
+        for (int np : P.classes) {
+            sms_of[np] = std::max(1, (int)std::lround(budget * sm_time[np] / sm_tot));
+            used += sms_of[np];
+        }
+        while (used > budget) {  // take the excess from the largest shares
+            int big = P.classes[0];
+            for (int np : P.classes)
+                if (sms_of[np] > sms_of[big]) big = np;
+            if (sms_of[big] <= 1) break;
+            --sms_of[big];
+            --used;
+        }
     }
     for (int np : P.classes) {
         const int NB = np / 8, G = R0_TAB_ITEMS[NB];
-        const long long full = (long long)std::max(1, ctx->persist_occ[NB]) * ctx->sms;
-        const int ctas = P.classes.size() == 1
-                             ? (int)full
-                             : (int)std::max<long long>(ctx->sms / 8, std::llround(full * work[np] / tot));
+        const int occ = std::max(1, ctx->persist_occ[NB]);
+        const int ctas = side ? sms_of[np] * occ : occ * ctx->sms;
         const int first = (int)P.pitems.size();
         int maxM = 0;
         for (const auto &pd : P.pairs)
@@ -255,6 +279,7 @@ void build_queue(bpmax_ctx *ctx, Plan &P)
             long long cells = 0;
             for (const auto &pd : P.pairs)
                 if (pd.Np == np && pd.M > d) cells += pd.M - d;
+            fin_items(d - 1);
             if (cells > 0 && P2 > 1) {  // offset pairs >= 1
                 const long long q = r0_pairs_per_job(cells, P2 - 1, ctas, qmin, std::max<long long>(P.pairs_per_job, qmin),
                                                      P.merge_items);
@@ -266,7 +291,6 @@ void build_queue(bpmax_ctx *ctx, Plan &P)
                                 P.prod_need[P.pairs[p].cell_base + cell_index(P.pairs[p].M, i1, i1 + d)] += 1;
                             }
             }
-            fin_items(d - 1);
             if (cells > 0)  // offset pair 0 (offsets 0 and d-1)
                 for (int p = 0; p < n; ++p)
                     if (P.pairs[p].Np == np && P.pairs[p].M > d)
@@ -692,12 +716,12 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         launches += 2;
     }
     const bool prof = kp && kp->on;
-    if (P.persistent) {  // one persistent launch per width class, side by side on the class streams
+    if (P.persistent) {  // one persistent launch per width class: side by side on the class streams, or in turn
         const int nclass = (int)P.pclasses.size();
         int *cnt = (int *)ctx->pcnt.p;
         int *diag_done = cnt + 64, *prod_done = diag_done + align64(P.n_counters);
         CK(cudaMemsetAsync(cnt, 0, ((size_t)64 + align64(P.n_counters) + P.prod_need.size()) * sizeof(int), ctx->stream));
-        const bool pfork = !prof && nclass > 1;
+        const bool pfork = !prof && nclass > 1 && P.persist == 1;
         if (pfork) {
             CK(cudaEventRecord(ctx->fork_ev, ctx->stream));
             for (int k = 0; k < std::min(nclass, MAX_CLASS_STREAMS); ++k)
@@ -1444,7 +1468,8 @@ int bpmax_gpu_set_tuning(bpmax_ctx *ctx, int key, long value)
         ctx->class_share = value != 0;
         break;
     case BPMAX_TUNE_PERSISTENT:
-        ctx->persist = value != 0;
+        if (value < 0 || value > 2) return fail(ctx, BPMAX_EINVAL, "persistent mode must be 0, 1 or 2");
+        ctx->persist = (int)value;
         break;
     default: return fail(ctx, BPMAX_EINVAL, "unknown tuning key %d", key);
     }
@@ -1525,9 +1550,10 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
     const Tuned sched = best_cfg;
     if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4], sched[5], 0});
     if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3, sched[5], 0});
-    if (!tiled && st == BPMAX_OK)  // the persistent fill, with the best pairs per job and merge cost
-        for (int jc : jobs_cand)
-            if (st == BPMAX_OK) try_cfg(Tuned{jc, sched[1], sched[2], 0, sched[4], 0, 1});
+    if (!tiled && st == BPMAX_OK)  // the persistent fill (classes side by side, then in turn), merge cost as found
+        for (int mode = 1; mode <= (classes.size() > 1 ? 2 : 1); ++mode)
+            for (int jc : jobs_cand)
+                if (st == BPMAX_OK) try_cfg(Tuned{jc, sched[1], sched[2], 0, sched[4], 0, mode});
     ctx->r0_pairs_per_job = saved[0];
     ctx->r0_merge_items = saved[1];
     ctx->class_streams = saved[2];

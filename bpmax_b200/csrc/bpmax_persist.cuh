@@ -17,10 +17,13 @@
 //     with the CTA's threads, writes the table, its S1 pieces and the SW1 push into the cleared
 //     table of (i1-1, i1+d+1), and counts itself in diag_done[pair][d].
 // The host orders the queue so that every item depends only on items before it: for d = 1, 2, ...
-// the jobs of diagonal d with p0 >= 1, then the finalize items of diagonal d-1, then the jobs of d
-// with p0 == 0; the finalize items of the last diagonal close the queue. Items are claimed in queue
-// order by running CTAs, so the earliest unfinished claimed item always has its dependencies
-// finished: the schedule makes progress whatever number of CTAs is resident.
+// the finalize items of diagonal d-1, then the jobs of diagonal d with p0 >= 1 (they run beside
+// those finalizes), then the jobs of d with p0 == 0; the finalize items of the last diagonal close
+// the queue. Items are claimed in queue order by running CTAs, one item ahead (a CTA claims its next
+// item while it works on the current one, and stages the item and its pair's descriptor in shared
+// memory, so the claim and those loads are off the critical path). The earliest unfinished claimed
+// item always has its dependencies finished, and its CTA has finished everything it claimed before
+// it: the schedule makes progress whatever number of CTAs is resident.
 // Publishing: every thread fences its writes (__threadfence), the CTA barrier joins them, and one
 // thread adds to the counter; the waiting thread reads the counter with ld.acquire.gpu, the CTA
 // barrier hands the result on, tables written by other CTAs are read with L2-only loads, and a
@@ -78,6 +81,8 @@ struct PersistCfg {
     static constexpr int FIN_BYTES = 2 * NP * NP * 4 + NP;                  // D, S2, bases (inside the ring)
     static_assert(FIN_BYTES <= C::OFF_RED, "the finalize's tables fit in the product's stages");
     static_assert(K <= 24, "slots");
+    static_assert(THREADS >= 64, "warp 1 claims the next item");
+    static_assert(sizeof(PItem) == 24 && sizeof(PairDesc) % 8 == 0 && sizeof(PairDesc) / 8 <= 32, "staged descriptors");
 };
 
 template <int NB>
@@ -95,7 +100,10 @@ fill_persistent_kernel(PersistCtl pc, const PairDesc *__restrict__ pairs, float 
     uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(psm) + C::OFF_BAR);
     int *done_cnt = reinterpret_cast<int *>(reinterpret_cast<char *>(psm) + C::OFF_CNT);
     int *armed = reinterpret_cast<int *>(reinterpret_cast<char *>(psm) + C::OFF_ARM);
-    __shared__ int item_sh, ok_sh;
+    __shared__ int ok_sh;
+    __shared__ int idx_sh[2];                             // claimed items, double-buffered
+    __shared__ int itm_sh[2][6];                          // their PItem
+    __shared__ long long pd_sh[2][sizeof(PairDesc) / 8];  // and their pair's descriptor
     __shared__ float s1_sh;
     __shared__ float wsh[12];
     __shared__ int cbs[NB];
@@ -132,16 +140,28 @@ fill_persistent_kernel(PersistCtl pc, const PairDesc *__restrict__ pairs, float 
     }
     const unsigned smem_base = smem_u32(psm);
     unsigned phase = 0;  // bit s: parity of stage s's next completion (kept across jobs)
+    // one full warp claims the next item and stages it and its pair's descriptor in slot t
+    auto claim = [&](int t) {
+        int nx = 0;
+        if (lane == 0) nx = atomicAdd(pc.head, 1);
+        nx = __shfl_sync(0xffffffffu, nx, 0);
+        if (lane == 0) idx_sh[t] = nx;
+        if (nx < pc.nitems) {
+            const int w = lane < 6 ? reinterpret_cast<const int *>(pc.items + nx)[lane] : 0;
+            if (lane < 6) itm_sh[t][lane] = w;
+            const int pr = __shfl_sync(0xffffffffu, w, 0);  // PItem::pair
+            if (lane < (int)(sizeof(PairDesc) / 8)) pd_sh[t][lane] = reinterpret_cast<const long long *>(pairs + pr)[lane];
+        }
+    };
+    if (warp == 0) claim(0);
     __syncthreads();
 
 #pragma unroll 1
-    while (true) {
-        if (tid == 0) item_sh = atomicAdd(pc.head, 1);
-        __syncthreads();
-        const int idx = item_sh;
+    for (int t = 0;; t ^= 1) {  // slot t holds the current item; the next one is claimed into t ^ 1
+        const int idx = idx_sh[t];
         if (idx >= pc.nitems) break;
-        const PItem itm = pc.items[idx];
-        const PairDesc pd = pairs[itm.pair];
+        const PItem itm = *reinterpret_cast<const PItem *>(itm_sh[t]);
+        const PairDesc pd = *reinterpret_cast<const PairDesc *>(pd_sh[t]);
         const int M = pd.M, d = itm.d, i1 = itm.i1, j1 = i1 + d;
         const long long cell = pd.cell_base + cell_index(M, i1, j1);
         // dependency wait (thread 0), its result to every thread
@@ -161,7 +181,9 @@ fill_persistent_kernel(PersistCtl pc, const PairDesc *__restrict__ pairs, float 
 
         if (itm.kind == 0) {
             // ---------------------------------------------------------------- product job
-            asm volatile("fence.proxy.async.global;" ::: "memory");  // tables of other CTAs before the bulk copies
+            // tables of other CTAs (global) and this CTA's finalize tables in the ring (shared), both
+            // written through the generic proxy, before the bulk copies (async proxy)
+            asm volatile("fence.proxy.async.global;\n\tfence.proxy.async.shared::cta;" ::: "memory");
             const R0Job job{itm.pair, i1, itm.p0, itm.p1};
             const int items = r0_job_items(job, d), iters = (items + C::G - 1) / C::G;
             const float *Fp = F + pd.F_off;
@@ -186,6 +208,7 @@ fill_persistent_kernel(PersistCtl pc, const PairDesc *__restrict__ pairs, float 
             __syncthreads();
             if (!ctl.inject)
                 for (int s = 0; s < prime; ++s) issue(s, s, tid, C::THREADS);
+            if (warp == 1) claim(t ^ 1);
             float acc[8][8];
 #pragma unroll
             for (int i = 0; i < 8; ++i)
@@ -277,6 +300,7 @@ fill_persistent_kernel(PersistCtl pc, const PairDesc *__restrict__ pairs, float 
         const uint8_t *s2r = bases + pd.seq2_off;
         float *D = psm, *S2s = psm + NP * NP;
         uint8_t *sb = reinterpret_cast<uint8_t *>(psm + 2 * NP * NP);
+        if (warp == 1) claim(t ^ 1);
         if (warp == 0) {  // S1(i1, j1) from the final S1 of shorter intervals (0 while j1 - i1 <= 3)
             float v = 0.0f;
             if (d > 3) {

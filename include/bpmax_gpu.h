@@ -129,11 +129,13 @@ int bpmax_gpu_grad_batch(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s,
  *                                most its share of the SMs (its share of the padded work, at least
  *                                1/16), so the classes' chains progress side by side; 0: every launch
  *                                may take every SM
- *   BPMAX_TUNE_PERSISTENT        1: fills whose strand-2 lengths are all <= 64 run as ONE persistent
- *                                launch per width class that walks the outer diagonals as a wavefront
- *                                with device-side dependency counters (bounded waits), the classes side
- *                                by side; 0: a graph of two launches per outer diagonal. The R0-only
- *                                mode and bpmax_gpu_fill's per-diagonal copy-out keep the graph. */
+ *   BPMAX_TUNE_PERSISTENT        1 or 2: fills whose strand-2 lengths are all <= 64 run as ONE
+ *                                persistent launch per width class that walks the outer diagonals as a
+ *                                wavefront with device-side dependency counters (bounded waits); with
+ *                                several width classes, 1 runs them side by side (each on its share of
+ *                                the SMs), 2 one after another (each on every SM); 0: a graph of two
+ *                                launches per outer diagonal. The R0-only mode and bpmax_gpu_fill's
+ *                                per-diagonal copy-out keep the graph. */
 enum bpmax_tuning_key {
     BPMAX_TUNE_R0_PAIRS_PER_JOB = 0,
     BPMAX_TUNE_R0_MERGE_ITEMS = 1,
@@ -156,7 +158,8 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value);
  * kernel shape (BPMAX_TUNE_R0_VARIANT 1, when a strand-2 length is <= 64) and the deeper tile ring
  * (BPMAX_TUNE_WIDE_STAGES 3, when one is in 65..320), after trying class shares
  * (BPMAX_TUNE_CLASS_SHARE 1, when class streams won with several width classes), then the persistent
- * fill with each pairs-per-job candidate (BPMAX_TUNE_PERSISTENT 1, when every strand-2 length is <= 64).
+ * fill with each pairs-per-job candidate (BPMAX_TUNE_PERSISTENT 1, and 2 with several width classes,
+ * when every strand-2 length is <= 64).
  * best (may be NULL) receives the 7 chosen values of keys 0, 1, 2, 6, 5, 7, 8 in that order; best_ms (may be NULL) the fill time in ms. Results of every
  * fill are unchanged by any setting (bit for bit). The reference's counterpart is choosing its tile
  * arguments N_tile, MR, NR by hand (V3/bpmax.c:129). */

@@ -1,8 +1,8 @@
 """The persistent fill (BPMAX_TUNE_PERSISTENT): one launch per width class walks the outer diagonals
 as a wavefront with device-side dependency counters instead of a graph of two launches per diagonal.
 Every result must equal the oracle's bit for bit: single pairs of every width class, uneven batches
-(several persistent launches side by side), repeated calls, and the timeout path (a wait that runs
-out ends the whole launch with BPMAX_ETIMEOUT and the context stays usable)."""
+(several persistent launches side by side, or one after another), repeated calls, and the timeout
+path (a wait that runs out ends the whole launch with BPMAX_ETIMEOUT and the context stays usable)."""
 import numpy as np
 import pytest
 
@@ -39,17 +39,39 @@ def test_persistent_single_pair_vs_oracle(eng, oracle_mod, M, N, seed, wkind):
     assert score == oracle_mod.score(Fo, M, N)
 
 
-def test_persistent_uneven_batch_vs_oracle(eng, oracle_mod):
+@pytest.mark.parametrize("mode", [1, 2])  # width classes side by side / one after another
+def test_persistent_uneven_batch_vs_oracle(eng, oracle_mod, mode):
     wl = W.batched_uneven(num_pairs=40, seed=123, m_range=(1, 45), n_range=(1, 64))
     eng.set_weights(wl.weights)
     exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, wl.weights)[0], len(a), len(b)) for a, b in wl.pairs],
                    dtype=np.float32)
-    for _ in range(2):  # the second call replays the captured graph
-        assert np.array_equal(bits(eng.score_batch(wl.pairs)), bits(exp))
-    for p in (0, 7, 39):
-        a, b = wl.pairs[p]
+    eng.set_tuning("persistent", mode)
+    try:
+        for _ in range(2):  # the second call replays the captured graph
+            assert np.array_equal(bits(eng.score_batch(wl.pairs)), bits(exp))
+        for p in (0, 7, 39):
+            a, b = wl.pairs[p]
+            win = eng.read_cells(p, 0, len(a), 0, len(a), len(b))
+            Fo, _, _ = oracle_mod.fill(a, b, wl.weights)
+            iu, ju = np.triu_indices(len(a))
+            assert np.array_equal(bits(win[iu, ju]), bits(Fo))
+    finally:
+        eng.set_tuning("persistent", 1)
+
+
+def test_persistent_batch_of_one_width_many_pairs(eng, oracle_mod):
+    """Many pairs of one width class in one launch: product and finalize ranges span pairs."""
+    rng = np.random.default_rng(9)
+    pairs = [W.pair(int(rng.integers(1, 60)), 24, 300 + k) for k in range(30)]
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    got = eng.score_batch(pairs)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
+                   dtype=np.float32)
+    assert np.array_equal(bits(got), bits(exp))
+    for p in (0, 11, 29):
+        a, b = pairs[p]
         win = eng.read_cells(p, 0, len(a), 0, len(a), len(b))
-        Fo, _, _ = oracle_mod.fill(a, b, wl.weights)
+        Fo, _, _ = oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)
         iu, ju = np.triu_indices(len(a))
         assert np.array_equal(bits(win[iu, ju]), bits(Fo))
 
