@@ -11,7 +11,8 @@ terms with C(n) = n(n^2-1)/6, T(n) = n(n+1)/2 (twice this is the reference's "bp
 With N GPUs every rank fills its own pair (independent pairs, no collective): weak scaling; a batched
 workload is split over the ranks by estimated work instead (strong scaling), its scores gathered once.
 The default line also carries the sub-measurements of the other configurations (batched pairs/s,
-the balanced 256 x 256 pair, the forward + adjoint batch), bitwise windows of the benched tables
+the balanced 256 x 256 pair, the forward + adjoint batch, the persistent fill against the graph of
+per-diagonal launches), bitwise windows of the benched tables
 against the reference's own fill ("parity"), and the reference's fill of a bounded sample timed on
 the host cores ("cpu_baseline").
 Prints ONE JSON line on rank 0.
@@ -393,6 +394,7 @@ def main_b200(args, world, rank, local):
         extra["batched"] = measure_batched(eng)
         extra["balanced"] = measure_balanced(eng, peak, with_reference=not args.no_cpu_baseline)
         extra["grad"] = measure_grad(eng)
+        extra["persistent"] = measure_persistent(local)
         eng.set_weights(wl.weights)
 
     if rank == 0:
@@ -536,6 +538,44 @@ def measure_batched(eng):
             "speedup_note": "speedup: summed device time of the per-pair fills (cached graphs) over the batched "
                             "fill's device time; speedup_wall: host wall clock of both passes, host work included",
             "autotuned": tuned, "autotune_best_ms": tune_ms}
+
+
+def measure_persistent(device: int):
+    """The persistent fill (one launch per width class walking the outer diagonals with device-side
+    dependency counters; the classes of a batch one after another) against the graph of per-diagonal
+    launches, on this GPU: median fill ms of three runs of each, single pairs and the 512-pair batch.
+    A separate engine, so that no autotuned schedule of the other measurements overrides the mode."""
+    from bpmax_b200 import Engine
+    e = Engine(device)
+    out = {}
+    try:
+        def med(f):
+            f()
+            runs = []
+            for _ in range(3):
+                f()
+                runs.append(e.last_timing()[0])
+            return statistics.median(runs)
+        e.set_weights(W.INTEGER_WEIGHTS)
+        for M, N in ((1024, 64), (200, 64), (200, 16)):
+            a, b = W.pair(M, N, 2)
+            r = {}
+            for mode, key in ((0, "graph_ms"), (1, "persistent_ms")):
+                e.set_tuning("persistent", mode)
+                r[key] = med(lambda: e.score(a, b))
+            r["speedup"] = r["graph_ms"] / r["persistent_ms"]
+            out[f"{M}x{N}"] = r
+        wl = W.batched_uneven(512, seed=4)
+        e.set_weights(wl.weights)
+        r = {}
+        for mode, key in ((0, "graph_ms"), (2, "persistent_ms")):
+            e.set_tuning("persistent", mode)
+            r[key] = med(lambda: e.score_batch(wl.pairs))
+        r["speedup"] = r["graph_ms"] / r["persistent_ms"]
+        out[wl.name] = r
+    finally:
+        e.close()
+    return out
 
 
 def measure_balanced(eng, peak, with_reference=True):
