@@ -97,6 +97,7 @@ struct Plan {
     // persistent fill (one launch per width class walking the diagonals with dependency counters):
     // the work queues of all classes back to back, each class's range and CTA count
     bool persistent = false, copyout = false;
+    RefOut ref{nullptr, 0, 0};  // finalize launches also write the reference layout (bpmax_gpu_fill)
     std::vector<PItem> pitems;
     struct PClass { int np, first, count, ctas; };
     std::vector<PClass> pclasses;
@@ -126,6 +127,8 @@ struct bpmax_ctx {
     DevBuf r0vals;         // R0-only mode: seq1 then seq2 of the pair, as floats
     DevBuf pq, pcnt, pneed;  // persistent fill: work queue; counters (class heads, diagonals, cells); jobs per cell
     bool copyout = false;    // the next fill copies the reference layout out per diagonal (graph path)
+    RefOut want_ref{nullptr, 0, 0};  // the next fill's finalize also writes the reference layout there
+    DevBuf refdev;                   // that reference layout, diagonal-major
     bool r0_only = false;  // mode of the next prepare()
     // schedule of the next prepare(): with the reference-layout copy-out running beside the fill
     // (bpmax_gpu_fill), the unsplit product leaves the SMs the row conversions need
@@ -580,7 +583,7 @@ void launch_fin_t(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
     finalize_small_kernel<8 * NB, T><<<L.count + (L.s1_count + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
         (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
         (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p, (const uint8_t *)ctx->bases.p, ctx->W,
-        L.d);
+        L.d, ctx->plan.ref);
 }
 
 template <int NB>
@@ -881,7 +884,9 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
     const bool same_tuning = ctx->plan.pairs_per_job == want[0] && ctx->plan.merge_items == want[1] &&
                              ctx->plan.class_streams == want[2] && ctx->plan.r0_variant == want[3] &&
                              ctx->plan.wide_stages == want[4] && ctx->plan.class_share == want[5] &&
-                             ctx->plan.persist == want[6] && ctx->plan.copyout == ctx->copyout;
+                             ctx->plan.persist == want[6] && ctx->plan.copyout == ctx->copyout &&
+                             ctx->plan.ref.out == ctx->want_ref.out && ctx->plan.ref.T == ctx->want_ref.T &&
+                             ctx->plan.ref.Ns == ctx->want_ref.Ns;
     if (!(ctx->plan_valid && ctx->plan.Ms == Ms && ctx->plan.Ns == Ns && same_tuning && ctx->plan.r0_only == ctx->r0_only &&
           ctx->plan.split == ctx->allow_split)) {
         if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
@@ -892,6 +897,7 @@ int prepare(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int> &
         if ((st = build_plan(ctx, Ms, Ns, ctx->plan)) != BPMAX_OK) return st;
         Plan &P = ctx->plan;
         P.r0_only = ctx->r0_only;
+        P.ref = ctx->want_ref;
         if (P.pairs.size() == 1) {
             P.diag_ev.assign(P.maxM, nullptr);
             for (auto &e : P.diag_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1149,7 +1155,7 @@ void bpmax_gpu_destroy(bpmax_ctx *ctx)
     if (ctx->plan.graph) cudaGraphExecDestroy(ctx->plan.graph);
     for (DevBuf *b : {&ctx->tbstack, &ctx->grads, &ctx->tbstatus, &ctx->F, &ctx->FT, &ctx->S, &ctx->bases, &ctx->pairs,
                       &ctx->r0jobs, &ctx->r0ljobs, &ctx->r0wjobs, &ctx->pq, &ctx->pcnt, &ctx->pneed, &ctx->celljobs,
-                      &ctx->scores, &ctx->conv, &ctx->errflag,
+                      &ctx->scores, &ctx->conv, &ctx->refdev, &ctx->errflag,
                       &ctx->r0vals})
         if (b->p) cudaFree(b->p);
     for (int i = 0; i < 2; ++i) {
@@ -1288,21 +1294,78 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
         return BPMAX_OK;
     }
     const long long cell_f = (long long)Ns * Ns * (N_tile + 1) * N_tile;
-    // outer row i1 of the reference layout: cells (i1, i1..M-1) are contiguous; it is final once
-    // outer diagonal M-1-i1 is, so rows are converted and copied out from the last one up while
-    // the fill still runs (aux stream, waiting on the per-diagonal events the graph records)
+    // The table is copied out while the fill still runs (aux stream, waiting on the per-diagonal
+    // events the graph records). Into pinned memory: per outer diagonal, as soon as it is final --
+    // its cells (i1, i1+d) lie (M+1) cells apart in the reference layout, so one strided copy
+    // places a diagonal converted into a staging slot, and the copy-out ends one diagonal after the
+    // fill. Into pageable memory (through a pinned staging buffer and a host copy): per outer row,
+    // contiguous in the layout and final once outer diagonal M-1-i1 is, from the last one up.
     const long long row_max = (long long)M * cell_f;
     int st;
     if ((st = ensure(ctx, ctx->conv, 2 * row_max * sizeof(float))) != BPMAX_OK) return st;
     const bool pinned = is_pinned(F_lin);
     if (!pinned && (st = ensure_host_stage(ctx, row_max * sizeof(float))) != BPMAX_OK) return st;
-    ctx->allow_split = false;
+    // Widths <= 64 into pinned memory: the finalize launches themselves write every cell they
+    // complete in the reference layout (diagonal-major, on the device), so only copy engines work
+    // beside the fill, which keeps its split schedule. Without room for that buffer, or wider,
+    // a conversion launch per diagonal does it (those launches share the SMs with the fill's,
+    // so the fill then runs unsplit).
+    const size_t fused_bytes = (size_t)(M * (M + 1) / 2) * cell_f * sizeof(float);
+    bool fused = false;
+    if (pinned && padded_width((int)N) <= MAX_SMALL_NP) {
+        fused = ctx->refdev.bytes >= fused_bytes;
+        if (!fused) {
+            if (ctx->refdev.p) cudaFree(ctx->refdev.p);
+            ctx->refdev = DevBuf{};
+            void *p = nullptr;
+            if (cudaMalloc(&p, fused_bytes) == cudaSuccess) {
+                ctx->refdev = DevBuf{p, fused_bytes};
+                fused = true;
+            } else {
+                cudaGetLastError();  // out of memory: not sticky, take the conversion launches
+            }
+        }
+    }
+    ctx->want_ref = fused ? RefOut{(float *)ctx->refdev.p, (int)N_tile, (int)Ns} : RefOut{nullptr, 0, 0};
+    ctx->allow_split = fused;
     ctx->copyout = true;
     st = fill_pairs(ctx, 1, &seq1, &M, &seq2, &N, true);
     ctx->allow_split = true;
     ctx->copyout = false;
+    ctx->want_ref = RefOut{nullptr, 0, 0};
     if (st != BPMAX_OK) return st;
     const std::vector<cudaEvent_t> &dev = ctx->plan.diag_ev;
+    if (fused) {
+        const size_t cell_b = (size_t)cell_f * sizeof(float);
+        for (long d = 0; d < M; ++d) {
+            const float *src = (const float *)ctx->refdev.p + (d * M - d * (d - 1) / 2) * cell_f;
+            CK(cudaStreamWaitEvent(ctx->aux_stream, dev[d], 0));
+            CK(cudaMemcpy2DAsync(F_lin + d * cell_f, (size_t)(M + 1) * cell_b, src, cell_b, cell_b, (size_t)(M - d),
+                                 cudaMemcpyDeviceToHost, ctx->aux_stream));
+        }
+        CK(cudaStreamSynchronize(ctx->aux_stream));
+        if ((st = finish_fill(ctx)) != BPMAX_OK) return st;
+        if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+        return BPMAX_OK;
+    }
+    if (pinned) {
+        const size_t cell_b = (size_t)cell_f * sizeof(float);
+        for (long d = 0; d < M; ++d) {
+            float *slot = (float *)ctx->conv.p + (d & 1) * row_max;
+            const long long n_out = (M - d) * cell_f;
+            CK(cudaStreamWaitEvent(ctx->aux_stream, dev[d], 0));
+            to_reference_diag_kernel<<<(int)std::min<long long>(4 * ctx->sms, (n_out + 255) / 256), 256, 0,
+                                       ctx->aux_stream>>>((const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p,
+                                                          (int)N_tile, (int)Ns, (int)d, n_out, slot);
+            CK(cudaGetLastError());
+            CK(cudaMemcpy2DAsync(F_lin + d * cell_f, (size_t)(M + 1) * cell_b, slot, cell_b, cell_b, (size_t)(M - d),
+                                 cudaMemcpyDeviceToHost, ctx->aux_stream));
+        }
+        CK(cudaStreamSynchronize(ctx->aux_stream));
+        if ((st = finish_fill(ctx)) != BPMAX_OK) return st;
+        if (score) CK(cudaMemcpy(score, ctx->scores.p, sizeof(float), cudaMemcpyDeviceToHost));
+        return BPMAX_OK;
+    }
     std::vector<long long> pending_n(2, 0);
     std::vector<float *> pending_dst(2, nullptr);
     for (long i1 = M - 1; i1 >= 0; --i1) {
@@ -1310,7 +1373,7 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
         float *dbuf = (float *)ctx->conv.p + slot * row_max;
         const long long n_out = (M - i1) * cell_f;
         float *dst = F_lin + (i1 * M + i1) * cell_f;
-        if (!pinned && pending_dst[slot]) {  // drain the staging buffer this slot used before
+        if (pending_dst[slot]) {  // drain the staging buffer this slot used before
             CK(cudaEventSynchronize(ctx->stage_ev[slot]));
             memcpy(pending_dst[slot], ctx->host_stage[slot], pending_n[slot] * sizeof(float));
             pending_dst[slot] = nullptr;
@@ -1319,18 +1382,13 @@ int bpmax_gpu_fill(bpmax_ctx *ctx, const int *seq1, long M, const int *seq2, lon
         to_reference_row_kernel<<<4 * ctx->sms, 256, 0, ctx->aux_stream>>>(
             (const PairDesc *)ctx->pairs.p, (const float *)ctx->F.p, (int)N_tile, (int)Ns, (int)i1, n_out, dbuf);
         CK(cudaGetLastError());
-        if (pinned) {
-            CK(cudaMemcpyAsync(dst, dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->aux_stream));
-        } else {
-            CK(cudaMemcpyAsync(ctx->host_stage[slot], dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost,
-                               ctx->aux_stream));
-            CK(cudaEventRecord(ctx->stage_ev[slot], ctx->aux_stream));
-            pending_dst[slot] = dst;
-            pending_n[slot] = n_out;
-        }
+        CK(cudaMemcpyAsync(ctx->host_stage[slot], dbuf, n_out * sizeof(float), cudaMemcpyDeviceToHost, ctx->aux_stream));
+        CK(cudaEventRecord(ctx->stage_ev[slot], ctx->aux_stream));
+        pending_dst[slot] = dst;
+        pending_n[slot] = n_out;
     }
     for (int slot = 0; slot < 2; ++slot)
-        if (!pinned && pending_dst[slot]) {
+        if (pending_dst[slot]) {
             CK(cudaEventSynchronize(ctx->stage_ev[slot]));
             memcpy(pending_dst[slot], ctx->host_stage[slot], pending_n[slot] * sizeof(float));
         }
@@ -1703,7 +1761,7 @@ void noalloc_launch_diag(cudaStream_t s, const NoallocDevice &nd, int d, int n_r
     const int n_s1 = n_cells - 1;  // S1 cells of diagonal d+1: the first n_cells-1 entries of cj
     using Sh = FinShape<8 * NB>;
     finalize_small_kernel<8 * NB><<<n_cells + (n_s1 + Sh::WARPS - 1) / Sh::WARPS, Sh::THREADS, Sh::SMEM, s>>>(
-        cj, n_cells, cj, n_s1, pd, F, S, bases, W, d);
+        cj, n_cells, cj, n_s1, pd, F, S, bases, W, d, RefOut{nullptr, 0, 0});
 }
 
 }  // namespace

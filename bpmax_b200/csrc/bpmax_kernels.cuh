@@ -222,6 +222,47 @@ struct CellJob {
 // threads per cell cost latency per cell but issue fewer instructions per step in total, which pays
 // when a launch holds many more cells than the GPU runs at once (FIN_WIDE_CELLS below)
 constexpr int fin_threads(int NP) { return NP >= 48 ? 512 : (NP >= 24 ? 256 : 64); }
+// element (r, c) of tile (I2, J2) of outer cell `cell` in the reference layout (tiles of T+1 rows,
+// the last one the halo; R = padding rows/columns of the first tile row/column)
+__device__ __forceinline__ float reference_tile_elem(const PairDesc &pd, const float *__restrict__ F, long long cell,
+                                                     int T, int R, int I2, int J2, int r, int c)
+{
+    const int Ri = I2 == 0 ? R : 0, Rj = (I2 == 0 && J2 == 0) ? R : 0;
+    float v = __int_as_float(0x7fc00000);  // NaN: a cell the reference leaves unwritten
+    if (I2 <= J2 && c >= Rj) {
+        if (r < T) {
+            if (r >= Ri) {
+                const int i2 = I2 * T + r - R, j2 = J2 * T + c - R;
+                v = i2 <= j2 ? f_value(pd, F, cell, i2, j2) : -3.402823466e+38f;
+            }
+        } else {
+            v = I2 == J2 ? -3.402823466e+38f : f_value(pd, F, cell, (I2 + 1) * T - R, J2 * T + c - R);
+        }
+    }
+    return v;
+}
+
+// element `rem` (in [0, Ns*Ns*(T+1)*T)) of outer cell (i1, j1) in the reference layout
+__device__ __forceinline__ float reference_elem(const PairDesc &pd, const float *__restrict__ F, int T, int Ns, int R,
+                                                int i1, int j1, long long rem)
+{
+    const long long tile_f = (long long)(T + 1) * T;
+    const int I2 = (int)(rem / ((long long)Ns * tile_f));
+    rem %= (long long)Ns * tile_f;
+    const int J2 = (int)(rem / tile_f);
+    rem %= tile_f;
+    return reference_tile_elem(pd, F, cell_index(pd.M, i1, j1), T, R, I2, J2, (int)(rem / T), (int)(rem % T));
+}
+
+// Reference-layout copy of the cells a finalize launch completes (the copy-out of bpmax_gpu_fill):
+// out == nullptr for none; else cell (i1, i1+d) of the (single) pair goes to
+// out + (d*M - d(d-1)/2 + i1) * cell_f, diagonal after diagonal, in the reference's tile layout of
+// N_tile = T (Ns tiles a side; see reference_elem)
+struct RefOut {
+    float *out;
+    int T, Ns;
+};
+
 constexpr int FIN_BULK_THREADS = 256;  // widths >= 48, launches of FIN_BULK_CELLS cells or more
 constexpr int FIN_BULK_CELLS = 2048;
 
@@ -250,7 +291,7 @@ template <int NP, int T = fin_threads(NP)>
 __global__ void __launch_bounds__(FinShape<NP, T>::THREADS, FinShape<NP, T>::MINB)
 finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
                       const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ S,
-                      const uint8_t *__restrict__ bases, Weights W, int d)
+                      const uint8_t *__restrict__ bases, Weights W, int d, RefOut ro)
 {
     using Sh = FinShape<NP, T>;
     constexpr int NB = NP / 8, NBLK = NB * (NB + 1) / 2, K = Sh::K;
@@ -383,6 +424,17 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
         if (h == 1) p.w = s1v;
         *reinterpret_cast<float4 *>(Fc + cbs[BJ] + 68 * (BJ + 1) + 4 * h) = p;
     }
+    if (ro.out) {  // this cell in the reference layout, from the image just written (visible to the CTA):
+        __syncthreads();  // one warp per tile row of T floats
+        const int TT = ro.T, R = (TT - N % TT) % TT, tile_rows = TT + 1, rows = ro.Ns * ro.Ns * tile_rows;
+        float *dst = ro.out + ((long long)d * M - (long long)d * (d - 1) / 2 + i1) * ((long long)rows * TT);
+        const long long cell = cell_index(M, i1, j1);
+        for (int rr = warp; rr < rows; rr += Sh::WARPS) {
+            const int I2 = rr / (ro.Ns * tile_rows), rem = rr % (ro.Ns * tile_rows);
+            const int J2 = rem / tile_rows, r = rem % tile_rows;
+            for (int c = lane; c < TT; c += 32) dst[rr * TT + c] = reference_tile_elem(pd, F, cell, TT, R, I2, J2, r, c);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -396,33 +448,25 @@ __global__ void to_reference_row_kernel(const PairDesc *__restrict__ pdp, const 
                                         int i1, long long n_out, float *__restrict__ out)
 {
     const PairDesc pd = *pdp;
-    const int M = pd.M, N = pd.N;
-    const int R = (T - N % T) % T;
-    const long long tile_f = (long long)(T + 1) * T;
-    const long long cell_f = (long long)Ns * Ns * tile_f;
+    const int R = (T - pd.N % T) % T;
+    const long long cell_f = (long long)Ns * Ns * (T + 1) * T;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n_out;
+         q += (long long)gridDim.x * blockDim.x)
+        out[q] = reference_elem(pd, F, T, Ns, R, i1, i1 + (int)(q / cell_f), q % cell_f);
+}
+
+// the same conversion for the cells of outer diagonal d (cells (i1, i1+d), i1 = 0 .. M-1-d), one
+// after another in `out`: final all at once when the diagonal is, unlike a row
+__global__ void to_reference_diag_kernel(const PairDesc *__restrict__ pdp, const float *__restrict__ F, int T, int Ns,
+                                         int d, long long n_out, float *__restrict__ out)
+{
+    const PairDesc pd = *pdp;
+    const int R = (T - pd.N % T) % T;
+    const long long cell_f = (long long)Ns * Ns * (T + 1) * T;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n_out;
          q += (long long)gridDim.x * blockDim.x) {
-        const int j1 = i1 + (int)(q / cell_f);
-        long long rem = q % cell_f;
-        const int I2 = (int)(rem / ((long long)Ns * tile_f));
-        rem %= (long long)Ns * tile_f;
-        const int J2 = (int)(rem / tile_f);
-        rem %= tile_f;
-        const int r = (int)(rem / T), c = (int)(rem % T);
-        const long long cell = cell_index(M, i1, j1);
-        const int Ri = I2 == 0 ? R : 0, Rj = (I2 == 0 && J2 == 0) ? R : 0;
-        float v = __int_as_float(0x7fc00000);  // NaN: a cell the reference leaves unwritten
-        if (I2 <= J2 && c >= Rj) {
-            if (r < T) {
-                if (r >= Ri) {
-                    const int i2 = I2 * T + r - R, j2 = J2 * T + c - R;
-                    v = i2 <= j2 ? f_value(pd, F, cell, i2, j2) : -3.402823466e+38f;
-                }
-            } else {
-                v = I2 == J2 ? -3.402823466e+38f : f_value(pd, F, cell, (I2 + 1) * T - R, J2 * T + c - R);
-            }
-        }
-        out[q] = v;
+        const int i1 = (int)(q / cell_f);
+        out[q] = reference_elem(pd, F, T, Ns, R, i1, i1 + d, q % cell_f);
     }
 }
 

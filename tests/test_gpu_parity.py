@@ -223,3 +223,39 @@ def test_tuning_rejects_bad_values(eng):
         eng.set_tuning("r0_pairs_per_job", 0)
     with pytest.raises(BpmaxError):
         eng._check(eng._L.bpmax_gpu_set_tuning(eng._ctx, 99, 1))
+
+
+@pytest.mark.parametrize("case", [c for c in G.cases() if "reference_layout_sha256" in c][:3], ids=lambda c: c["name"])
+def test_golden_reference_layout_pinned(eng, case, oracle_mod):
+    """Into pinned host memory the table is copied out per outer diagonal (one strided copy each)
+    instead of per row: same golden digest, the same NaN below the diagonal, and the same bytes as
+    the pageable path."""
+    import torch
+
+    s1, s2, w = G.decode(case["seq1"]), G.decode(case["seq2"]), G.weights(case)
+    M, N, T = case["M"], case["N"], case["N_tile"]
+    eng.set_weights(w)
+    n = eng.reference_size(M, N, T)
+    buf = torch.full((n,), float("nan"), dtype=torch.float32, pin_memory=True)
+    Fp, score = eng.fill(s1, s2, T, out=buf.numpy())
+    mask = oracle_mod.reference_written_mask(M, N, T)
+    assert score == case["score"]
+    assert G.sha(Fp[mask]) == case["reference_layout_sha256"]
+    Fr, _ = eng.fill(s1, s2, T)
+    assert np.array_equal(bits(Fp), bits(Fr))  # NaN patterns included
+
+
+def test_reference_layout_pinned_vs_oracle(eng, oracle_mod):
+    import torch
+
+    M, N, T = 70, 64, 32
+    s1, s2 = W.pair(M, N, 71)
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    n = eng.reference_size(M, N, T)
+    buf = torch.full((n,), float("nan"), dtype=torch.float32, pin_memory=True)
+    Fp, _ = eng.fill(s1, s2, T, out=buf.numpy())
+    Fo, _, _ = oracle_mod.fill(s1, s2, W.INTEGER_WEIGHTS)
+    mask = oracle_mod.reference_written_mask(M, N, T)
+    assert np.array_equal(bits(oracle_mod.to_reference_layout(Fo, M, N, T)[mask]), bits(Fp[mask]))
+    lower = np.tril(np.ones((M, M), dtype=bool), -1)
+    assert np.isnan(Fp.reshape(M, M, -1)[lower]).all()
