@@ -222,10 +222,11 @@ struct CellJob {
 // threads per cell cost latency per cell but issue fewer instructions per step in total, which pays
 // when a launch holds many more cells than the GPU runs at once (FIN_WIDE_CELLS below)
 constexpr int fin_threads(int NP) { return NP >= 48 ? 512 : (NP >= 24 ? 256 : 64); }
-// element (r, c) of tile (I2, J2) of outer cell `cell` in the reference layout (tiles of T+1 rows,
-// the last one the halo; R = padding rows/columns of the first tile row/column)
-__device__ __forceinline__ float reference_tile_elem(const PairDesc &pd, const float *__restrict__ F, long long cell,
-                                                     int T, int R, int I2, int J2, int r, int c)
+// element (r, c) of tile (I2, J2) of an outer cell in the reference layout (tiles of T+1 rows, the
+// last one the halo; R = padding rows/columns of the first tile row/column); val(i2, j2) gives the
+// cell's inner value for 0 <= i2 <= j2 < N, the only entries read
+template <class Val>
+__device__ __forceinline__ float reference_tile_elem_v(const Val &val, int T, int R, int I2, int J2, int r, int c)
 {
     const int Ri = I2 == 0 ? R : 0, Rj = (I2 == 0 && J2 == 0) ? R : 0;
     float v = __int_as_float(0x7fc00000);  // NaN: a cell the reference leaves unwritten
@@ -233,13 +234,18 @@ __device__ __forceinline__ float reference_tile_elem(const PairDesc &pd, const f
         if (r < T) {
             if (r >= Ri) {
                 const int i2 = I2 * T + r - R, j2 = J2 * T + c - R;
-                v = i2 <= j2 ? f_value(pd, F, cell, i2, j2) : -3.402823466e+38f;
+                v = i2 <= j2 ? val(i2, j2) : -3.402823466e+38f;
             }
         } else {
-            v = I2 == J2 ? -3.402823466e+38f : f_value(pd, F, cell, (I2 + 1) * T - R, J2 * T + c - R);
+            v = I2 == J2 ? -3.402823466e+38f : val((I2 + 1) * T - R, J2 * T + c - R);
         }
     }
     return v;
+}
+__device__ __forceinline__ float reference_tile_elem(const PairDesc &pd, const float *__restrict__ F, long long cell,
+                                                     int T, int R, int I2, int J2, int r, int c)
+{
+    return reference_tile_elem_v([&](int i2, int j2) { return f_value(pd, F, cell, i2, j2); }, T, R, I2, J2, r, c);
 }
 
 // element `rem` (in [0, Ns*Ns*(T+1)*T)) of outer cell (i1, j1) in the reference layout
@@ -424,15 +430,15 @@ finalize_small_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
         if (h == 1) p.w = s1v;
         *reinterpret_cast<float4 *>(Fc + cbs[BJ] + 68 * (BJ + 1) + 4 * h) = p;
     }
-    if (ro.out) {  // this cell in the reference layout, from the image just written (visible to the CTA):
-        __syncthreads();  // one warp per tile row of T floats
+    if (ro.out) {  // this cell in the reference layout, from the final table in shared memory (the
+                   // values the image holds), one warp per tile row of T floats
         const int TT = ro.T, R = (TT - N % TT) % TT, tile_rows = TT + 1, rows = ro.Ns * ro.Ns * tile_rows;
         float *dst = ro.out + ((long long)d * M - (long long)d * (d - 1) / 2 + i1) * ((long long)rows * TT);
-        const long long cell = cell_index(M, i1, j1);
+        auto dval = [&](int i2, int j2) { return D[(j2 - i2) * NP + i2]; };
         for (int rr = warp; rr < rows; rr += Sh::WARPS) {
             const int I2 = rr / (ro.Ns * tile_rows), rem = rr % (ro.Ns * tile_rows);
             const int J2 = rem / tile_rows, r = rem % tile_rows;
-            for (int c = lane; c < TT; c += 32) dst[rr * TT + c] = reference_tile_elem(pd, F, cell, TT, R, I2, J2, r, c);
+            for (int c = lane; c < TT; c += 32) dst[rr * TT + c] = reference_tile_elem_v(dval, TT, R, I2, J2, r, c);
         }
     }
 }
