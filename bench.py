@@ -47,6 +47,8 @@ def parse_args():
     ap.add_argument("--workload", default="single", choices=["single", "small", "balanced", "batched", "grad"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched pairs/s sub-measurement")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="batches: keep the default schedule (no autotuner runs before the warm-up steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--pair", default=None, help="M,N: one custom uniform pair instead of the workload")
     ap.add_argument("--r0-only", default=None, metavar="M,N",
@@ -338,7 +340,7 @@ def main_b200(args, world, rank, local):
         return eng.last_timing()
 
     tuned = None
-    if not single:  # batches: schedule chosen by the autotuner on these shapes (outside the timing)
+    if not single and not args.no_autotune:  # batches: schedule chosen by the autotuner on these shapes (untimed)
         tuned, _ = eng.autotune(my_pairs, trials=1)
     for _ in range(max(args.warmup, 0)):
         step()
