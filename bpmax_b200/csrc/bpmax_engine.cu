@@ -1608,10 +1608,11 @@ int bpmax_gpu_autotune(bpmax_ctx *ctx, int num_pairs, const int *const *seq1s, c
     const Tuned sched = best_cfg;
     if (small && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], 1, sched[4], sched[5], 0});
     if (tiled && st == BPMAX_OK) try_cfg(Tuned{sched[0], sched[1], sched[2], best_cfg[3], 3, sched[5], 0});
-    if (!tiled && st == BPMAX_OK)  // the persistent fill (classes side by side, then in turn), merge cost as found
-        for (int mode = 1; mode <= (classes.size() > 1 ? 2 : 1); ++mode)
-            for (int jc : jobs_cand)
-                if (st == BPMAX_OK) try_cfg(Tuned{jc, sched[1], sched[2], 0, sched[4], 0, mode});
+    // the persistent fill, merge cost as found; several width classes one after another (side by side,
+    // mode 1, they do not stay on their SM shares and measured 4.5x slower on the 512-pair batch)
+    if (!tiled && st == BPMAX_OK)
+        for (int jc : jobs_cand)
+            if (st == BPMAX_OK) try_cfg(Tuned{jc, sched[1], sched[2], 0, sched[4], 0, classes.size() > 1 ? 2 : 1});
     ctx->r0_pairs_per_job = saved[0];
     ctx->r0_merge_items = saved[1];
     ctx->class_streams = saved[2];

@@ -158,7 +158,7 @@ int bpmax_gpu_get_tuning(const bpmax_ctx *ctx, int key, long *value);
  * kernel shape (BPMAX_TUNE_R0_VARIANT 1, when a strand-2 length is <= 64) and the deeper tile ring
  * (BPMAX_TUNE_WIDE_STAGES 3, when one is in 65..320), after trying class shares
  * (BPMAX_TUNE_CLASS_SHARE 1, when class streams won with several width classes), then the persistent
- * fill with each pairs-per-job candidate (BPMAX_TUNE_PERSISTENT 1, and 2 with several width classes,
+ * fill with each pairs-per-job candidate (BPMAX_TUNE_PERSISTENT 1, or 2 with several width classes,
  * when every strand-2 length is <= 64).
  * best (may be NULL) receives the 7 chosen values of keys 0, 1, 2, 6, 5, 7, 8 in that order; best_ms (may be NULL) the fill time in ms. Results of every
  * fill are unchanged by any setting (bit for bit). The reference's counterpart is choosing its tile
