@@ -62,7 +62,12 @@ int bpmax_gpu_shim_set_weights(const float *weights12);
  * (logical cells, -FLT_MAX below the diagonal of diagonal tiles and in their halo row, and the
  * halo row of off-diagonal tiles = row 0 of the tile below). Cells the reference leaves
  * unwritten inside outer cells i1<=j1 (tiles with I2>J2, padding rows and columns) receive NaN;
- * outer cells i1>j1 are not touched. F_lin may be pinned (cudaHostAlloc) for direct copies.
+ * outer cells i1>j1 are not touched. The table is copied out while the fill runs. With F_lin
+ * pinned (cudaHostAlloc) and N <= 64, the fill also writes each cell in the reference layout into a
+ * device buffer of the table's size, kept by the context for later calls (freed by
+ * bpmax_gpu_destroy), and one strided copy per outer diagonal moves it to F_lin; without device
+ * memory for it, or with N > 64, conversion launches per diagonal do it. A pageable F_lin is filled
+ * row by row through pinned staging buffers.
  * score (may be NULL) receives F(0,M-1,0,N-1). Preconditions as the reference
  * (V3/bpmax.c:131): M>=1, N>=8, N_tile>=4, N_sec>=2, 0<=R<N_tile.
  * Replaces V3/bpmax.c:129 (the tiling arguments MR, NR, P only tune the CPU code). */
