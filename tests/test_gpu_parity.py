@@ -259,3 +259,21 @@ def test_reference_layout_pinned_vs_oracle(eng, oracle_mod):
     assert np.array_equal(bits(oracle_mod.to_reference_layout(Fo, M, N, T)[mask]), bits(Fp[mask]))
     lower = np.tril(np.ones((M, M), dtype=bool), -1)
     assert np.isnan(Fp.reshape(M, M, -1)[lower]).all()
+
+
+def test_wide_reference_layout_pinned(eng, oracle_mod):
+    """Pinned output with a strand-2 length over 64: one conversion launch and one strided copy per
+    outer diagonal; the same bytes as the pageable path and the oracle's cells."""
+    import torch
+
+    M, N, T = 9, 150, 64
+    s1, s2 = W.pair(M, N, 58)
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    n = eng.reference_size(M, N, T)
+    buf = torch.full((n,), float("nan"), dtype=torch.float32, pin_memory=True)
+    Fp, _ = eng.fill(s1, s2, T, out=buf.numpy())
+    Fr, _ = eng.fill(s1, s2, T)
+    assert np.array_equal(bits(Fp), bits(Fr))
+    Fo, _, _ = oracle_mod.fill(s1, s2, W.INTEGER_WEIGHTS)
+    mask = oracle_mod.reference_written_mask(M, N, T)
+    assert np.array_equal(bits(oracle_mod.to_reference_layout(Fo, M, N, T)[mask]), bits(Fp[mask]))
