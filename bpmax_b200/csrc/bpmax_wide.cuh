@@ -75,40 +75,64 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
     auto job_items = [&](const R0JobW &jb) {
         return r0_job_items(R0Job{jb.pair, jb.i1, jb.p0, jb.p1}, d) * ((jb.tile & 0xff) - (jb.tile >> 8) + 1);
     };
-    // arms stage s for item n of job j and issues its two copies (one thread)
-    auto fill_stage = [&](int s, int j, int n) {
-        const R0JobW jb = jobs[j];
-        const PairDesc pd = pairs[jb.pair];
-        const int BI = jb.tile >> 8, BJ = jb.tile & 0xff, nkb = BJ - BI + 1, KB = BI + n % nkb, NT = pd.Np >> 6;
+    // the producer's current job and its pair's M, Np and F_off, one copy per warp in shared memory,
+    // refreshed when the warp's producer position moves to another job (as in r0_kernel: no
+    // dependent global loads per refill)
+    __shared__ R0JobW pjob_sh[C::WARPS];
+    __shared__ long long pfoff_sh[C::WARPS];
+    __shared__ int pm_sh[C::WARPS], pnp_sh[C::WARPS];
+    const int warp_id = tid >> 5;
+    auto load_pjob = [&](int j_) {
+        __syncwarp();  // every lane of the warp is done with the previous copy
+        if (lane == 0) {
+            const R0JobW jb = jobs[j_];
+            pjob_sh[warp_id] = jb;
+            pm_sh[warp_id] = pairs[jb.pair].M;
+            pnp_sh[warp_id] = pairs[jb.pair].Np;
+            pfoff_sh[warp_id] = pairs[jb.pair].F_off;
+        }
+        __syncwarp();
+    };
+    // arms stage s for item n of the producer's job (the warp's copy) and issues its two copies
+    // (one thread)
+    auto fill_stage = [&](int s, int n) {
+        const R0JobW jb = pjob_sh[warp_id];
+        const int M = pm_sh[warp_id];
+        const int BI = jb.tile >> 8, BJ = jb.tile & 0xff, nkb = BJ - BI + 1, KB = BI + n % nkb, NT = pnp_sh[warp_id] >> 6;
         const int k1 = jb.i1 + r0_item_offset(R0Job{jb.pair, jb.i1, jb.p0, jb.p1}, d, n / nkb);
         const int j1 = jb.i1 + d;
         const long long CELL = wide_cell_floats(NT);
-        const float *Fp = F + pd.F_off;
+        const float *Fp = F + pfoff_sh[warp_id];
         const unsigned bar = smem_u32(bars + s);
         const int ab = 16 * (KB == BI ? WIDE_DIAG_CHUNKS : WIDE_DENSE_CHUNKS);
         const int bb = 16 * (KB == BJ ? WIDE_DIAG_CHUNKS : WIDE_DENSE_CHUNKS);
         mbar_arrive_tx(bar, (unsigned)(ab + bb));
         armed[s] += 1;
         const unsigned dst = smem_base + (unsigned)(s * C::STAGE_BYTES);
-        bulk_g2s(dst, Fp + cell_index(pd.M, jb.i1, k1) * CELL + wide_tile_off(NT, BI, KB), (unsigned)ab, bar);
-        bulk_g2s(dst + 16 * C::SLOT, Fp + cell_index(pd.M, k1 + 1, j1) * CELL + wide_tile_off(NT, KB, BJ), (unsigned)bb,
+        bulk_g2s(dst, Fp + cell_index(M, jb.i1, k1) * CELL + wide_tile_off(NT, BI, KB), (unsigned)ab, bar);
+        bulk_g2s(dst + 16 * C::SLOT, Fp + cell_index(M, k1 + 1, j1) * CELL + wide_tile_off(NT, KB, BJ), (unsigned)bb,
                  bar);
     };
 
     // consumer position (job jid, item it of items) and producer position S items ahead
     int items = job_items(jobs[jid]), it = 0;
     int pj = jid, pit = 0, pitems = items;
-    auto advance = [&](int &j_, int &items_, int &it_) {
-        if (++it_ >= items_) {
-            it_ = 0;
-            j_ += gridDim.x;
-            if (j_ < njobs) items_ = job_items(jobs[j_]);
+    // the producer's advance (every warp the same way) also refreshes the warp's copy of its job
+    auto advance_p = [&]() {
+        if (++pit >= pitems) {
+            pit = 0;
+            pj += gridDim.x;
+            if (pj < njobs) {
+                pitems = job_items(jobs[pj]);
+                load_pjob(pj);
+            }
         }
     };
+    load_pjob(pj);
     for (int s = 0; s < S; ++s)
         if (pj < njobs) {
-            if (tid == 0 && !ctl.inject) fill_stage(s, pj, pit);
-            advance(pj, pitems, pit);
+            if (tid == 0 && !ctl.inject) fill_stage(s, pit);
+            advance_p();
         }
 
     // the lane's task: DD jobs use the width-64 kernel's lane table and warp programs (task (bi, bj,
@@ -197,10 +221,10 @@ r0_wide_kernel(const R0JobW *__restrict__ jobs, int njobs, const PairDesc *__res
             const bool refill = pj < njobs && !__any_sync(0xffffffffu, bad);  // (test mode: every warp is bad)
             if (lane == 0) {
                 done_cnt[stage] = 0;
-                if (refill) fill_stage(stage, pj, pit);
+                if (refill) fill_stage(stage, pit);
             }
         }
-        if (pj < njobs) advance(pj, pitems, pit);
+        if (pj < njobs) advance_p();
         if (++kbi > BJ - BI) kbi = 0;
         if (++it >= items) {  // job done: merge the partial maxima into the output tile
             const R0JobW job = jobs[jid];
