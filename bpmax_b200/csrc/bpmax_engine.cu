@@ -350,7 +350,7 @@ int build_plan(bpmax_ctx *ctx, const std::vector<int> &Ms, const std::vector<int
         pd.S2t_off = s;
         s = align64(s + (long long)pd.Np * pd.Np);
         pd.S2d_off = s;
-        if (pd.Np > MAX_SMALL_NP) s = align64(s + (long long)pd.Np * pd.Np);
+        if (pd.Np > MAX_SMALL_NP) s = align64(s + (long long)pd.Np * (pd.Np + 1) / 2);  // triangular S2D
         pd.seq1_off = b;
         b += Ms[p];
         pd.seq2_off = b;

@@ -53,7 +53,7 @@ struct PairDesc {
     long long S2_off;  // float offset of S2 in the S arena
     long long S2m_off; // Np > 64 only: S2 with -inf outside its triangle
     long long S2t_off; // Np > 64 only: ST1[j][k] = S2(k+1, j), -inf outside
-    long long S2d_off; // Np > 64 only: S2 diagonal-major, S2D[e][i] = S2(i, i+e), -inf outside
+    long long S2d_off; // Np > 64 only: S2 diagonal-major and triangular, S2(i, i+e) at drow(Np, e) + i, -inf outside
     int seq1_off;      // offset of seq1 in the base arena (uint8)
     int seq2_off;      // offset of the REVERSED seq2 in the base arena (uint8)
     long long cell_base;  // persistent fill: index of the pair's cell (0, 0) among all pairs' cells

@@ -63,8 +63,10 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // Rearranged copies of S2 (S2 over the reversed strand 2, V3/bpmax_verify.c:560-571) for the wide
 // inner wavefronts (Np > 64): the masked S2M[i][k] = S2(i,k) if i <= k < N else -inf and
 // ST1[j][k] = S2(k+1,j) if k+1 <= j < N else -inf (global-memory wavefront), and the
-// diagonal-major S2D[e][i] = S2(i, i+e) if i+e < N else -inf (shared-memory wavefront). One CTA
-// per pair; pairs of the cell-image widths have nothing to do.
+// triangular diagonal-major S2D: row e holds S2(i, i+e) for i = 0 .. Np-1-e (-inf where i+e >= N) at
+// drow(Np, e) + i (shared-memory wavefront; T(Np) floats, half the square copy, so more of it stays
+// in L1 beside the wavefront's shared-memory table). One CTA per pair; pairs of the cell-image widths
+// have nothing to do.
 // ------------------------------------------------------------------------------------------
 __global__ void s2_aux_kernel(const PairDesc *__restrict__ pairs, float *__restrict__ S)
 {
@@ -77,7 +79,7 @@ __global__ void s2_aux_kernel(const PairDesc *__restrict__ pairs, float *__restr
         const int r = q / Np, c = q % Np;
         S2M[q] = (r <= c && c < N) ? S2[q] : NEG_INF;
         ST1[q] = (c + 1 <= r && r < N) ? S2[(c + 1) * Np + r] : NEG_INF;
-        S2D[q] = c + r < N ? S2[c * Np + c + r] : NEG_INF;  // r = e, c = i
+        if (c < Np - r) S2D[drow(Np, r) + c] = c + r < N ? S2[c * Np + c + r] : NEG_INF;  // r = e, c = i
     }
 }
 
@@ -438,7 +440,7 @@ finalize_wide_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob 
         const float *De = D + drow(Np, e);
         for (int e2 = e + 1 + warp; e2 < N; e2 += WARPS) {
             float *Dw = D + drow(Np, e2);
-            const float *S2r = S2D + (long long)(e2 - e - 1) * Np;
+            const float *S2r = S2D + drow(Np, e2 - e - 1);
             const bool fin = e2 == e + 1 && e2 >= 4;
             const float *Dp = D + drow(Np, max(e2 - 2, 0)) + 1;
             for (int i2 = lane; i2 < N - e2; i2 += 32) {
