@@ -531,21 +531,39 @@ void launch_r0_wide(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaSt
         launch_r0_wide_t<2>(ctx, L, s);
 }
 
-void launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
+// the finalize of one launch of cells wider than 64; returns the number of kernel launches
+int launch_fin_large(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaStream_t s)
 {
+    const CellJob *jobs = (const CellJob *)ctx->celljobs.p + L.first;
+    const CellJob *s1jobs = (const CellJob *)ctx->celljobs.p + L.s1_first;
+    const PairDesc *pairs = (const PairDesc *)ctx->pairs.p;
+    const uint8_t *bases = (const uint8_t *)ctx->bases.p;
+    float *F = (float *)ctx->F.p, *S = (float *)ctx->S.p;
     if (L.np <= FIN_WIDE_MAX_NP) {
         constexpr int WW = FIN_WIDE_THREADS / 32;
         finalize_wide_kernel<<<L.count + (L.s1_count + WW - 1) / WW, FIN_WIDE_THREADS, fin_wide_smem(L.np), s>>>(
-            (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first,
-            L.s1_count, (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->S.p,
-            (const uint8_t *)ctx->bases.p, ctx->W, L.d);
-        return;
+            jobs, L.count, s1jobs, L.s1_count, pairs, F, S, bases, ctx->W, L.d);
+        return 1;
     }
-    constexpr int W = FIN_LARGE_THREADS / 32;
-    finalize_large_kernel<<<L.count + (L.s1_count + W - 1) / W, FIN_LARGE_THREADS, 0, s>>>(
-        (const CellJob *)ctx->celljobs.p + L.first, L.count, (const CellJob *)ctx->celljobs.p + L.s1_first, L.s1_count,
-        (const PairDesc *)ctx->pairs.p, (float *)ctx->F.p, (float *)ctx->FT.p, (float *)ctx->S.p,
-        (const uint8_t *)ctx->bases.p, ctx->W, L.d);
+    // row-major tables: start values, then one launch per inner diagonal over every cell, then the
+    // SW1 pushes, the S1 slots and S1 of diagonal d+1
+    float *FT = (float *)ctx->FT.p;
+    int nmax = 0;  // longest strand 2 among the launch's cells
+    for (int q = 0; q < L.count; ++q) nmax = std::max(nmax, P.pairs[P.cell_jobs[L.first + q].pair].N);
+    const int nt = L.np / 32;
+    if (L.count > 0)
+        large_init_kernel<<<dim3(nt * nt, L.count), dim3(32, 8), 0, s>>>(jobs, pairs, F, FT, S, bases, ctx->W, L.d);
+    int n = L.count > 0 ? 1 : 0;
+    for (int dd = 1; dd < nmax && L.count > 0; ++dd, ++n) {
+        const long long warps = (long long)L.count * (nmax - dd);
+        large_step_kernel<<<(unsigned)((warps + 7) / 8), 256, 0, s>>>(jobs, L.count, pairs, F, FT, S, bases, ctx->W,
+                                                                      L.d, dd, nmax);
+    }
+    const long long tile = (long long)L.np * L.np;
+    const int chunks = (int)((tile + LARGE_FINAL_CHUNK - 1) / LARGE_FINAL_CHUNK);
+    large_final_kernel<<<L.count * chunks + (L.s1_count + 7) / 8, 256, 0, s>>>(jobs, L.count, chunks, s1jobs, L.s1_count,
+                                                                             pairs, F, FT, S, bases, ctx->W, L.d);
+    return n + 1;
 }
 
 template <int NB, int V>
@@ -715,6 +733,11 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
         ProfScope ps(ctx, kp, 0);
         single_strand_kernel<<<(int)P.pairs.size(), 512, 0, ctx->stream>>>(
             (const PairDesc *)ctx->pairs.p, (const uint8_t *)ctx->bases.p, (float *)ctx->S.p, ctx->W);
+        for (int p = 0; p < (int)P.pairs.size(); ++p)  // wider tables: one launch per diagonal of S2
+            if (P.pairs[p].Np > WIDE_TILE_MAX_NP)
+                for (int d = 4; d < P.pairs[p].N; ++d, ++launches)
+                    s2_diag_kernel<<<(P.pairs[p].N - d + 7) / 8, 256, 0, ctx->stream>>>(
+                        (const PairDesc *)ctx->pairs.p, p, (const uint8_t *)ctx->bases.p, (float *)ctx->S.p, ctx->W, d);
         s2_aux_kernel<<<(int)P.pairs.size(), 256, 0, ctx->stream>>>((const PairDesc *)ctx->pairs.p, (float *)ctx->S.p);
         launches += 2;
     }
@@ -838,7 +861,7 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
                     launch_r0only_fin(ctx, L, st);
                 } else {
                     switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-                    case 0: launch_fin_large(ctx, L, st); break;
+                    case 0: launches += launch_fin_large(ctx, P, L, st) - 1; break;
                     case 1: launch_fin<1>(ctx, L, st); break;
                     case 2: launch_fin<2>(ctx, L, st); break;
                     case 3: launch_fin<3>(ctx, L, st); break;

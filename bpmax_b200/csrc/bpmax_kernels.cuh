@@ -154,12 +154,14 @@ __device__ __forceinline__ float f_value(const PairDesc &pd, const float *__rest
 // Single-strand table S2 over the reversed strand 2 (V3/bpmax_verify.c:560-571):
 // S(i,j) = 0 if j-i<=3, else max(S(i+1,j-1)+intra(s[i],s[j]), max_{i<=k<j} S(i,k)+S(k+1,j)).
 // One CTA per pair; wavefront over the diagonal j-i. Cells outside the N x N upper triangle are
-// left at 0 and never read. (S1 is built diagonal by diagonal inside finalize_small_kernel.)
+// left at 0 and never read. (S1 is built diagonal by diagonal inside finalize_small_kernel.) Pairs
+// with tables wider than the tile images are left to s2_diag_kernel, one launch per diagonal.
 // ------------------------------------------------------------------------------------------
 __global__ void single_strand_kernel(const PairDesc *__restrict__ pairs, const uint8_t *__restrict__ bases,
                                      float *__restrict__ S, Weights W)
 {
     const PairDesc pd = pairs[blockIdx.x];
+    if (pd.Np > WIDE_TILE_MAX_NP) return;  // row-major tables: one launch per diagonal (s2_diag_kernel)
     const bool second = true;
     const int L = second ? pd.N : pd.M;
     const int ld = second ? pd.Np : pd.M;

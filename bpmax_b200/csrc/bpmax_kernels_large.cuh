@@ -263,23 +263,101 @@ r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__re
 }
 
 // ------------------------------------------------------------------------------------------
-// Finalize for Np > 64: one CTA per outer cell of diagonal d, inner wavefront over the cell's
-// tables in global memory (L2-resident). Same candidates as finalize_small_kernel:
-//   base inter, S1+S2, SW1 (already in F, pushed two diagonals earlier), SW2, R1, R2;
-// F and FT are kept consistent during the wavefront so R2 reads rows of FT.
-// CTAs after the first njobs compute S1 on diagonal d+1, one warp per cell.
+// Inner wavefront for Np > FIN_WIDE_MAX_NP (row-major F and its transpose FT, Np x Np per outer
+// cell, in global memory), spread over the whole GPU: the outer cells of diagonal d are finalized
+// together, one launch per inner diagonal dd, the launch boundary being the wavefront's barrier, so
+// every SM works on every inner step. (One CTA per outer cell walking its N-1 steps alone used at
+// most M-d SMs: a 16x3000 fill took 87 s in it.) Same candidates as finalize_small_kernel: base
+// inter, S1+S2, SW1 (already in F, pushed two diagonals earlier), SW2, R1, R2.
+//   large_init_kernel   start values of every entry of F, and FT, through 32x32 shared tiles
+//   large_step_kernel   inner diagonal dd of every outer cell: one warp per inner cell
+//   large_final_kernel  the SW1 push into (i1-1, j1+1), S1 on the subdiagonal of F and the
+//                       superdiagonal of FT; CTAs after the cells' compute S1 on diagonal d+1
 // ------------------------------------------------------------------------------------------
-constexpr int FIN_LARGE_THREADS = 512;
+constexpr int LARGE_FINAL_CHUNK = 8192;  // table entries per CTA of large_final_kernel
 
-__global__ void __launch_bounds__(FIN_LARGE_THREADS)
-finalize_large_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob *__restrict__ s1jobs, int ns1,
-                      const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
-                      float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
+// grid (Np/32)^2 tiles x cells, block 32 x 8
+__global__ void __launch_bounds__(256)
+large_init_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restrict__ pairs, float *__restrict__ F,
+                  float *__restrict__ FT, const float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W,
+                  int d)
 {
-    constexpr int NT = FIN_LARGE_THREADS, WARPS = NT / 32;
+    __shared__ float tl[32][33];
+    const CellJob job = jobs[blockIdx.y];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1, j1 = i1 + d;
+    const int nt = Np >> 5, tr = (int)blockIdx.x / nt, tc = (int)blockIdx.x % nt;
+    const long long tile = (long long)Np * Np;
+    float *Fc = F + pd.F_off + cell_index(M, i1, j1) * tile;
+    float *FTc = FT + pd.F_off + cell_index(M, i1, j1) * tile;
+    const float *S2 = S + pd.S2_off;
+    const float s1v = S[pd.S1_off + i1 * M + j1];
+    const uint8_t *s1 = bases + pd.seq1_off, *s2r = bases + pd.seq2_off;
+    const int x = threadIdx.x;
+    for (int y = threadIdx.y; y < 32; y += 8) {
+        const int r = 32 * tr + y, c = 32 * tc + x;
+        const long long q = (long long)r * Np + c;
+        float v = NEG_INF;
+        if (r <= c && c < N) v = (d == 0 && r == c) ? score_w(W.w + 6, s1[i1], s2r[r]) : fmaxf(Fc[q], s1v + S2[q]);
+        Fc[q] = v;
+        tl[y][x] = v;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += 8)  // FT[c][r] = F[r][c]: row 32tc+y, columns 32tr+x
+        FTc[(long long)(32 * tc + y) * Np + 32 * tr + x] = tl[x][y];
+}
+
+// one warp per inner cell (i2, i2+dd) of each of the ncells outer cells; warp w takes i2 = w / ncells
+// of outer cell w % ncells, so the warps of one i2 (and one pair) read the same S2 rows
+__global__ void __launch_bounds__(256)
+large_step_kernel(const CellJob *__restrict__ jobs, int ncells, const PairDesc *__restrict__ pairs,
+                  float *__restrict__ F, float *__restrict__ FT, const float *__restrict__ S,
+                  const uint8_t *__restrict__ bases, Weights W, int d, int dd, int nmax)
+{
+    const long long w = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const long long i2l = w / ncells;
+    if (i2l >= nmax - dd) return;  // (warp-uniform, as every return below)
+    const CellJob job = jobs[(int)(w % ncells)];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1;
+    const int i2 = (int)i2l, j2 = i2 + dd;
+    if (j2 >= N) return;
+    const long long tile = (long long)Np * Np;
+    const long long cell = cell_index(M, i1, i1 + d);
+    float *Fc = F + pd.F_off + cell * tile;
+    float *FTc = FT + pd.F_off + cell * tile;
+    const float *fr = Fc + (long long)i2 * Np, *sr = S + pd.S2m_off + (long long)i2 * Np;
+    const float *str = S + pd.S2t_off + (long long)j2 * Np, *ftr = FTc + (long long)j2 * Np + 1;
+    float r0 = NEG_INF, r1 = NEG_INF;
+    int k = i2 + lane;
+    for (; k + 32 < j2; k += 64) {
+        r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
+        r1 = fmax3(r1, fr[k + 32] + str[k + 32], sr[k + 32] + ftr[k + 32]);
+    }
+    if (k < j2) r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
+    float red = fmaxf(r0, r1);
+    for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
+    if (lane == 0) {
+        const uint8_t *s2r = bases + pd.seq2_off;
+        float v = fmaxf(Fc[(long long)i2 * Np + j2], red);
+        if (dd >= 4) v = fmaxf(v, Fc[(long long)(i2 + 1) * Np + (j2 - 1)] + score_w(W.w, s2r[i2], s2r[j2]));
+        Fc[(long long)i2 * Np + j2] = v;
+        FTc[(long long)j2 * Np + i2] = v;
+    }
+}
+
+// CTAs [0, ncells * chunks): entries [chunk * LARGE_FINAL_CHUNK, ...) of one outer cell; after them,
+// one warp per S1 cell (i, i+d+1)
+__global__ void __launch_bounds__(256)
+large_final_kernel(const CellJob *__restrict__ jobs, int ncells, int chunks, const CellJob *__restrict__ s1jobs,
+                   int ns1, const PairDesc *__restrict__ pairs, float *__restrict__ F, float *__restrict__ FT,
+                   float *__restrict__ S, const uint8_t *__restrict__ bases, Weights W, int d)
+{
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if ((int)blockIdx.x >= njobs) {  // S1 cells (i, i+d+1), one per warp
-        const int q = ((int)blockIdx.x - njobs) * WARPS + warp;
+    const int b = (int)blockIdx.x;
+    if (b >= ncells * chunks) {  // S1 cells (i, i+d+1), one per warp
+        const int q = (b - ncells * chunks) * 8 + warp;
         if (q >= ns1) return;
         const CellJob job = s1jobs[q];
         const PairDesc pd = pairs[job.pair];
@@ -293,77 +371,64 @@ finalize_large_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
         if (lane == 0) S1[i * M + j] = fmaxf(S1[(i + 1) * M + (j - 1)] + score_w(W.w, s1[i], s1[j]), red);
         return;
     }
-    const CellJob job = jobs[blockIdx.x];
+    const int ch = b % chunks;
+    const CellJob job = jobs[b / chunks];
     const PairDesc pd = pairs[job.pair];
     const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1, j1 = i1 + d;
     const long long tile = (long long)Np * Np;
     float *Fc = F + pd.F_off + cell_index(M, i1, j1) * tile;
     float *FTc = FT + pd.F_off + cell_index(M, i1, j1) * tile;
-    const float *S1 = S + pd.S1_off;
-    const float *S2 = S + pd.S2_off;
-    const float *S2M = S + pd.S2m_off;
-    const float *ST1 = S + pd.S2t_off;
-    const uint8_t *s1 = bases + pd.seq1_off;
-    const uint8_t *s2r = bases + pd.seq2_off;
-    const float s1v = S1[i1 * M + j1];
-    for (long long q = tid; q < tile; q += NT) {
-        const int r = (int)(q / Np), c = (int)(q % Np);
-        float v = NEG_INF;
-        if (r <= c && c < N) v = (d == 0 && r == c) ? score_w(W.w + 6, s1[i1], s2r[r]) : fmaxf(Fc[q], s1v + S2[q]);
-        Fc[q] = v;
-    }
-    __syncthreads();
-    for (long long q = tid; q < tile; q += NT) {
-        const int r = (int)(q / Np), c = (int)(q % Np);
-        FTc[q] = Fc[(long long)c * Np + r];
-    }
-    __syncthreads();
-    for (int dd = 1; dd < N; ++dd) {
-        const int cells = N - dd;
-        int g = 1;
-        while (g < 32 && g * 2 * cells <= NT) g *= 2;
-        const int lane_g = tid & (g - 1);
-        const int slots = NT / g;
-        for (int base = 0; base < cells; base += slots) {
-            const int i2 = base + tid / g, j2 = i2 + dd;
-            const bool act = i2 < cells;
-            float r0 = NEG_INF, r1 = NEG_INF;
-            if (act) {
-                const float *fr = Fc + (long long)i2 * Np, *sr = S2M + (long long)i2 * Np;
-                const float *str = ST1 + (long long)j2 * Np, *ftr = FTc + (long long)j2 * Np + 1;
-                int k = i2 + lane_g;
-                for (; k + g < j2; k += 2 * g) {
-                    r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
-                    r1 = fmax3(r1, fr[k + g] + str[k + g], sr[k + g] + ftr[k + g]);
-                }
-                if (k < j2) r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
-            }
-            float red = fmaxf(r0, r1);
-            for (int o = g >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o, g));
-            if (act && lane_g == 0) {
-                float v = fmaxf(Fc[(long long)i2 * Np + j2], red);
-                if (dd >= 4)
-                    v = fmaxf(v, Fc[(long long)(i2 + 1) * Np + (j2 - 1)] + score_w(W.w, s2r[i2], s2r[j2]));
-                Fc[(long long)i2 * Np + j2] = v;
-                FTc[(long long)j2 * Np + i2] = v;
-            }
-        }
-        __syncthreads();
-    }
-    // SW1 candidate of cell (i1-1, j1+1), whose table nothing else has written yet
+    const float s1v = S[pd.S1_off + i1 * M + j1];
+    // SW1 candidate of cell (i1-1, j1+1), whose table nothing else has written yet (entries r <= c;
+    // the subdiagonal written below is not among them)
     if (i1 >= 1 && j1 + 1 < M && d + 2 >= 4) {
+        const uint8_t *s1 = bases + pd.seq1_off;
         const float wp = score_w(W.w, s1[i1 - 1], s1[j1 + 1]);
         float *Fn = F + pd.F_off + cell_index(M, i1 - 1, j1 + 1) * tile;
-        for (long long q = tid; q < tile; q += NT) {
+        const long long q1 = min(tile, (long long)(ch + 1) * LARGE_FINAL_CHUNK);
+        for (long long q = (long long)ch * LARGE_FINAL_CHUNK + tid; q < q1; q += 256) {
             const int r = (int)(q / Np), c = (int)(q % Np);
             Fn[q] = (r <= c && c < N) ? Fc[q] + wp : 0.0f;
         }
     }
-    __syncthreads();
-    // S1(i1,j1) on the subdiagonal of F (and the superdiagonal of FT): the R3/R4 slots
-    for (int r = 1 + tid; r < Np; r += NT) {
-        Fc[(long long)r * Np + r - 1] = s1v;
-        FTc[(long long)(r - 1) * Np + r] = s1v;
+    if (ch == 0)  // S1(i1,j1) on the subdiagonal of F (and the superdiagonal of FT): the R3/R4 slots
+        for (int r = 1 + tid; r < Np; r += 256) {
+            Fc[(long long)r * Np + r - 1] = s1v;
+            FTc[(long long)(r - 1) * Np + r] = s1v;
+        }
+}
+
+// ------------------------------------------------------------------------------------------
+// S2 (V3/bpmax_verify.c:560-571) of one pair with Np > FIN_WIDE_MAX_NP, one launch per diagonal d of
+// its wavefront (single_strand_kernel's one CTA per pair took 2.2 s at N = 3000), one warp per cell.
+// The column operand S2(k+1, j) is read from ST1[j][k], which the same launches fill as cells become
+// final (s2_aux_kernel rewrites ST1 completely afterwards); S starts at 0, so ST1 holds the 0 of
+// every cell with j-i <= 3.
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+s2_diag_kernel(const PairDesc *__restrict__ pairs, int p, const uint8_t *__restrict__ bases, float *__restrict__ S,
+               Weights W, int d)
+{
+    const PairDesc pd = pairs[p];
+    const int L = pd.N, ld = pd.Np;
+    const int i = (int)blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= L - d) return;
+    const int j = i + d;
+    float *T = S + pd.S2_off, *TT = S + pd.S2t_off;
+    const uint8_t *s = bases + pd.seq2_off;
+    float r0 = NEG_INF, r1 = NEG_INF;
+    int k = i + lane;
+    for (; k + 32 < j; k += 64) {
+        r0 = fmaxf(r0, T[(long long)i * ld + k] + TT[(long long)j * ld + k]);
+        r1 = fmaxf(r1, T[(long long)i * ld + k + 32] + TT[(long long)j * ld + k + 32]);
+    }
+    if (k < j) r0 = fmaxf(r0, T[(long long)i * ld + k] + TT[(long long)j * ld + k]);
+    float red = fmaxf(r0, r1);
+    for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
+    if (lane == 0) {
+        const float v = fmaxf(T[(long long)(i + 1) * ld + (j - 1)] + score_w(W.w, s[i], s[j]), red);
+        T[(long long)i * ld + j] = v;
+        if (i >= 1) TT[(long long)j * ld + i - 1] = v;
     }
 }
 
@@ -384,6 +449,7 @@ finalize_large_kernel(const CellJob *__restrict__ jobs, int njobs, const CellJob
 // ------------------------------------------------------------------------------------------
 constexpr int FIN_WIDE_THREADS = 1024;
 constexpr int FIN_WIDE_MAX_NP = 320;  // T(320) floats = 205,440 bytes of shared memory
+static_assert(FIN_WIDE_MAX_NP == WIDE_TILE_MAX_NP, "tables wider than the tile images are the row-major ones");
 
 __host__ __device__ constexpr size_t fin_wide_smem(int Np) { return (size_t)Np * (Np + 1) / 2 * 4 + Np; }
 

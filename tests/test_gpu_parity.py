@@ -154,6 +154,29 @@ def test_wide_inner_tables_vs_oracle(eng, oracle_mod, M, N, seed, wkind):
     assert score == oracle_mod.score(Fo, M, N)
 
 
+@pytest.mark.parametrize("M,N,seed,wkind", [(4, 330, 71, "int"), (3, 400, 72, "real"), (6, 343, 73, "int")])
+def test_row_major_inner_tables_vs_oracle(eng, oracle_mod, M, N, seed, wkind):
+    """Strand-2 lengths above 320 take the row-major tables: S2 by one launch per diagonal, the
+    blocked product with its transposed copy, and the inner wavefront as one launch per inner
+    diagonal over every cell of the outer diagonal."""
+    s1, s2 = W.pair(M, N, seed)
+    w = W.INTEGER_WEIGHTS if wkind == "int" else W.random_weights(seed)
+    eng.set_weights(w)
+    F, score = eng.fill_compact(s1, s2)
+    Fo, _, _ = oracle_mod.fill(s1, s2, w)
+    assert np.array_equal(bits(F), bits(Fo))
+    assert score == oracle_mod.score(Fo, M, N)
+
+
+def test_row_major_inner_tables_in_a_batch(eng, oracle_mod):
+    pairs = [W.pair(m, n, 80 + i) for i, (m, n) in enumerate([(4, 330), (7, 40), (3, 352), (5, 100)])]
+    eng.set_weights(W.INTEGER_WEIGHTS)
+    got = eng.score_batch(pairs)
+    exp = np.array([oracle_mod.score(oracle_mod.fill(a, b, W.INTEGER_WEIGHTS)[0], len(a), len(b)) for a, b in pairs],
+                   dtype=np.float32)
+    assert np.array_equal(bits(got), bits(exp))
+
+
 def test_wide_inner_reference_layout(eng, oracle_mod):
     M, N, T = 6, 150, 64
     s1, s2 = W.pair(M, N, 57)
