@@ -545,19 +545,24 @@ int launch_fin_large(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaS
             jobs, L.count, s1jobs, L.s1_count, pairs, F, S, bases, ctx->W, L.d);
         return 1;
     }
-    // row-major tables: start values, then one launch per inner diagonal over every cell, then the
-    // SW1 pushes, the S1 slots and S1 of diagonal d+1
+    // row-major tables: start values, then per tile diagonal t the products over finished tiles and
+    // the tiles' own wavefronts, then the SW1 pushes, the S1 slots and S1 of diagonal d+1
+    (void)P;
     float *FT = (float *)ctx->FT.p;
-    int nmax = 0;  // longest strand 2 among the launch's cells
-    for (int q = 0; q < L.count; ++q) nmax = std::max(nmax, P.pairs[P.cell_jobs[L.first + q].pair].N);
-    const int nt = L.np / 32;
-    if (L.count > 0)
-        large_init_kernel<<<dim3(nt * nt, L.count), dim3(32, 8), 0, s>>>(jobs, pairs, F, FT, S, bases, ctx->W, L.d);
-    int n = L.count > 0 ? 1 : 0;
-    for (int dd = 1; dd < nmax && L.count > 0; ++dd, ++n) {
-        const long long warps = (long long)L.count * (nmax - dd);
-        large_step_kernel<<<(unsigned)((warps + 7) / 8), 256, 0, s>>>(jobs, L.count, pairs, F, FT, S, bases, ctx->W,
-                                                                      L.d, dd, nmax);
+    const int nt32 = L.np / 32, NT = L.np / LT;
+    int n = 0;
+    if (L.count > 0) {
+        large_init_kernel<<<dim3(nt32 * nt32, L.count), dim3(32, 8), 0, s>>>(jobs, pairs, F, FT, S, bases, ctx->W, L.d);
+        ++n;
+        for (int t = 0; t < NT; ++t) {
+            if (t > 0) {
+                large_tile_product_kernel<<<dim3(NT - t, L.count), 256, 0, s>>>(jobs, pairs, F, FT, S, L.d, t);
+                ++n;
+            }
+            large_tile_local_kernel<<<dim3(NT - t, L.count), 256, LARGE_LOCAL_SMEM, s>>>(jobs, pairs, F, FT, S, bases,
+                                                                                         ctx->W, L.d, t);
+            ++n;
+        }
     }
     const long long tile = (long long)L.np * L.np;
     const int chunks = (int)((tile + LARGE_FINAL_CHUNK - 1) / LARGE_FINAL_CHUNK);
@@ -686,6 +691,8 @@ int set_smem_attr(bpmax_ctx *ctx)
         CK(cudaFuncSetAttribute(r0_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WideShape::SMEM));
         CK(cudaFuncSetAttribute(finalize_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)fin_wide_smem(FIN_WIDE_MAX_NP)));
+        CK(cudaFuncSetAttribute(large_tile_local_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)LARGE_LOCAL_SMEM));
     }
     return BPMAX_OK;
 }

@@ -264,15 +264,26 @@ r0_large_kernel(const R0JobL *__restrict__ jobs, int njobs, const PairDesc *__re
 
 // ------------------------------------------------------------------------------------------
 // Inner wavefront for Np > FIN_WIDE_MAX_NP (row-major F and its transpose FT, Np x Np per outer
-// cell, in global memory), spread over the whole GPU: the outer cells of diagonal d are finalized
-// together, one launch per inner diagonal dd, the launch boundary being the wavefront's barrier, so
-// every SM works on every inner step. (One CTA per outer cell walking its N-1 steps alone used at
-// most M-d SMs: a 16x3000 fill took 87 s in it.) Same candidates as finalize_small_kernel: base
+// cell, in global memory), spread over the whole GPU and blocked in 64x64 tiles. The outer cells of
+// diagonal d are finalized together. Tile (I, J) of F (rows 64I.., columns 64J..) needs
+//   R1  F[i2][k] + S2(k+1, j2), k in [i2, j2): k < 64J lies in the finished tiles (I, K), K < J;
+//       k >= 64J in the tile itself
+//   R2  S2(i2, k) + F[k+1][j2], k+1 in (i2, j2]: k+1 >= 64(I+1) lies in the finished tiles (K, J),
+//       K > I; k+1 < 64(I+1) in the tile itself
+// so the tiles are done by tile diagonal t = J - I: first the terms over finished tiles as max-plus
+// tile products (large_tile_product_kernel, t >= 1), then the tile's own terms, SW2 and its final
+// values by a local wavefront over the tile's diagonals b - a in shared memory
+// (large_tile_local_kernel). Every launch covers the tiles of diagonal t of every outer cell, and
+// the launch boundaries are the only barriers (2 Np/64 + 1 launches per outer diagonal). The
+// entries below the diagonal and past N are -inf in F and in the masked copies S2M, ST1, so the
+// products need no bounds of their own. (One CTA per outer cell walking all N-1 inner steps used
+// at most M-d SMs: a 16x3000 fill took 87 s in it.) Same candidates as finalize_small_kernel: base
 // inter, S1+S2, SW1 (already in F, pushed two diagonals earlier), SW2, R1, R2.
-//   large_init_kernel   start values of every entry of F, and FT, through 32x32 shared tiles
-//   large_step_kernel   inner diagonal dd of every outer cell: one warp per inner cell
-//   large_final_kernel  the SW1 push into (i1-1, j1+1), S1 on the subdiagonal of F and the
-//                       superdiagonal of FT; CTAs after the cells' compute S1 on diagonal d+1
+//   large_init_kernel          start values of every entry of F, and FT, through 32x32 tiles
+//   large_tile_product_kernel  the R1/R2 terms over finished tiles, merged into F
+//   large_tile_local_kernel    the tile's own R1/R2 terms and SW2, then F and FT of the tile
+//   large_final_kernel         the SW1 push into (i1-1, j1+1), S1 on the subdiagonal of F and the
+//                              superdiagonal of FT; CTAs after the cells' compute S1 on diagonal d+1
 // ------------------------------------------------------------------------------------------
 constexpr int LARGE_FINAL_CHUNK = 8192;  // table entries per CTA of large_final_kernel
 
@@ -307,43 +318,142 @@ large_init_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restrict__
         FTc[(long long)(32 * tc + y) * Np + 32 * tr + x] = tl[x][y];
 }
 
-// one warp per inner cell (i2, i2+dd) of each of the ncells outer cells; warp w takes i2 = w / ncells
-// of outer cell w % ncells, so the warps of one i2 (and one pair) read the same S2 rows
+constexpr int LT = 64;       // tile side
+constexpr int LT_LD = 66;    // shared row stride of the product's operand slabs (8-byte pairs, conflict-free)
+constexpr int LT_LD1 = 65;   // shared row stride of the local wavefront's tables
+constexpr size_t LARGE_LOCAL_SMEM = 3 * LT * LT_LD1 * sizeof(float);
+
+// grid (NT - t) x cells, 256 threads (16 x 16): tile (I, I+t) of each outer cell. Thread (tx, ty)
+// owns outputs a = ty + 16u, b = tx + 16v (u, v < 4). Slabs of 64 k: R1 with A = F rows i2 and
+// B = ST1 rows j2 over k in [64K, 64K+64), K = I .. J-1; R2 with A = S2M rows i2 over
+// k = 64K-1 .. 64K+62 and B = FT rows j2 over k+1 = 64K .. 64K+63, K = I+1 .. J. Candidates are added
+// in k pairs: (A[a][k], A[a][k+1]) + (B[b][k], B[b][k+1]), both neighbouring words of a slab row.
 __global__ void __launch_bounds__(256)
-large_step_kernel(const CellJob *__restrict__ jobs, int ncells, const PairDesc *__restrict__ pairs,
-                  float *__restrict__ F, float *__restrict__ FT, const float *__restrict__ S,
-                  const uint8_t *__restrict__ bases, Weights W, int d, int dd, int nmax)
+large_tile_product_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restrict__ pairs, float *__restrict__ F,
+                          const float *__restrict__ FT, const float *__restrict__ S, int d, int t)
 {
-    const long long w = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    const long long i2l = w / ncells;
-    if (i2l >= nmax - dd) return;  // (warp-uniform, as every return below)
-    const CellJob job = jobs[(int)(w % ncells)];
+    __shared__ __align__(16) float As[LT * LT_LD];
+    __shared__ __align__(16) float Bs[LT * LT_LD];
+    const CellJob job = jobs[blockIdx.y];
     const PairDesc pd = pairs[job.pair];
-    const int M = pd.M, N = pd.N, Np = pd.Np, i1 = job.i1;
-    const int i2 = (int)i2l, j2 = i2 + dd;
-    if (j2 >= N) return;
-    const long long tile = (long long)Np * Np;
-    const long long cell = cell_index(M, i1, i1 + d);
+    const int M = pd.M, N = pd.N, Np = pd.Np, I = (int)blockIdx.x, J = I + t;
+    if (LT * I >= N || LT * J >= N) return;  // the tile lies past the table (CTA-uniform)
+    const long long tile = (long long)Np * Np, cell = cell_index(M, job.i1, job.i1 + d);
+    float *Fc = F + pd.F_off + cell * tile;
+    const float *FTc = FT + pd.F_off + cell * tile;
+    const float *S2M = S + pd.S2m_off, *ST1 = S + pd.S2t_off;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    float acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = NEG_INF;
+    // slab q: q < t is R1 with K = I + q, q >= t is R2 with K = I + 1 + (q - t)
+    for (int q = 0; q < 2 * t; ++q) {
+        const bool r1 = q < t;
+        const int K = r1 ? I + q : I + 1 + (q - t);
+        const float *A = r1 ? Fc : S2M;            // rows 64I + a
+        const float *B = r1 ? ST1 : FTc;           // rows 64J + b
+        const int ka = r1 ? LT * K : LT * K - 1;   // first column of the A slab
+        const int kb = LT * K;                     // first column of the B slab
+        __syncthreads();  // the previous slab is no longer read
+        for (int e = tid; e < LT * LT; e += 256) {
+            const int r = e >> 6, c = e & 63;
+            As[r * LT_LD + c] = A[(long long)(LT * I + r) * Np + ka + c];
+            Bs[r * LT_LD + c] = B[(long long)(LT * J + r) * Np + kb + c];
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < LT; k += 2) {
+            float2 av[4], bv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) av[u] = *reinterpret_cast<const float2 *>(As + (ty + 16 * u) * LT_LD + k);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) bv[v] = *reinterpret_cast<const float2 *>(Bs + (tx + 16 * v) * LT_LD + k);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const float2 sm = __fadd2_rn(av[u], bv[v]);
+                    acc[u][v] = fmax3(acc[u][v], sm.x, sm.y);
+                }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int i2 = LT * I + ty + 16 * u, j2 = LT * J + tx + 16 * v;
+            if (i2 <= j2 && j2 < N) {
+                float *f = Fc + (long long)i2 * Np + j2;
+                *f = fmaxf(*f, acc[u][v]);
+            }
+        }
+}
+
+// grid (NT - t) x cells, 256 threads: tile (I, I+t) of each outer cell, local coordinates
+// (a, b) = (i2 - 64I, j2 - 64J). An entry depends on the entries left of it in its tile row (R1),
+// below it in its tile column (R2) and at (a+1, b-1) (SW2), so the tile's diagonals b - a are done
+// in increasing order, one CTA barrier each, four threads per entry:
+//   R1  T[a][b'] + S2(64J+b'+1, 64J+b),   b' < b     (ST1 block rows 64J+b, columns 64J+b')
+//   R2  S2(64I+a, 64I+a'-1) + T[a'][b],   a' > a     (S2M block rows 64I+a, columns 64I+a'-1)
+// (on a diagonal tile the terms outside b' >= a, a' <= b meet a -inf entry below the diagonal).
+// T starts with F's values after the tile product (start values, SW1, R0/R3/R4, terms over
+// finished tiles); at the end F and FT take the tile.
+__global__ void __launch_bounds__(256)
+large_tile_local_kernel(const CellJob *__restrict__ jobs, const PairDesc *__restrict__ pairs, float *__restrict__ F,
+                        float *__restrict__ FT, const float *__restrict__ S, const uint8_t *__restrict__ bases,
+                        Weights W, int d, int t)
+{
+    extern __shared__ float ltl[];      // LARGE_LOCAL_SMEM bytes
+    float *Tt = ltl;                    // the tile
+    float *Sj = ltl + LT * LT_LD1;      // Sj[b][b'] = ST1[64J+b][64J+b'] = S2(64J+b'+1, 64J+b)
+    float *Si = ltl + 2 * LT * LT_LD1;  // Si[a][c] = S2M[64I+a][64I+c] = S2(64I+a, 64I+c)
+    const CellJob job = jobs[blockIdx.y];
+    const PairDesc pd = pairs[job.pair];
+    const int M = pd.M, N = pd.N, Np = pd.Np, I = (int)blockIdx.x, J = I + t;
+    if (LT * I >= N || LT * J >= N) return;  // the tile lies past the table (CTA-uniform)
+    const long long tile = (long long)Np * Np, cell = cell_index(M, job.i1, job.i1 + d);
     float *Fc = F + pd.F_off + cell * tile;
     float *FTc = FT + pd.F_off + cell * tile;
-    const float *fr = Fc + (long long)i2 * Np, *sr = S + pd.S2m_off + (long long)i2 * Np;
-    const float *str = S + pd.S2t_off + (long long)j2 * Np, *ftr = FTc + (long long)j2 * Np + 1;
-    float r0 = NEG_INF, r1 = NEG_INF;
-    int k = i2 + lane;
-    for (; k + 32 < j2; k += 64) {
-        r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
-        r1 = fmax3(r1, fr[k + 32] + str[k + 32], sr[k + 32] + ftr[k + 32]);
+    const float *S2M = S + pd.S2m_off, *ST1 = S + pd.S2t_off;
+    const uint8_t *s2r = bases + pd.seq2_off;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < LT * LT; e += 256) {
+        const int r = e >> 6, c = e & 63;
+        Tt[r * LT_LD1 + c] = Fc[(long long)(LT * I + r) * Np + LT * J + c];
+        Sj[r * LT_LD1 + c] = ST1[(long long)(LT * J + r) * Np + LT * J + c];
+        Si[r * LT_LD1 + c] = S2M[(long long)(LT * I + r) * Np + LT * I + c];
     }
-    if (k < j2) r0 = fmax3(r0, fr[k] + str[k], sr[k] + ftr[k]);
-    float red = fmaxf(r0, r1);
-    for (int o = 16; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));
-    if (lane == 0) {
-        const uint8_t *s2r = bases + pd.seq2_off;
-        float v = fmaxf(Fc[(long long)i2 * Np + j2], red);
-        if (dd >= 4) v = fmaxf(v, Fc[(long long)(i2 + 1) * Np + (j2 - 1)] + score_w(W.w, s2r[i2], s2r[j2]));
-        Fc[(long long)i2 * Np + j2] = v;
-        FTc[(long long)j2 * Np + i2] = v;
+    __syncthreads();
+    const int g = tid & 3, slot = tid >> 2;  // four threads per entry, 64 entries per step
+    for (int l = (t == 0 ? 1 : -(LT - 1)); l < LT; ++l) {
+        const int a = l >= 0 ? slot : slot - l, b = a + l;  // entry slot of tile diagonal l
+        const int i2 = LT * I + a, j2 = LT * J + b;
+        const bool act = a < LT && b < LT && b >= 0 && i2 <= j2 && j2 < N;
+        float red = NEG_INF;
+        if (act) {
+            for (int bp = g; bp < b; bp += 4) red = fmaxf(red, Tt[a * LT_LD1 + bp] + Sj[b * LT_LD1 + bp]);
+            for (int ap = a + 1 + g; ap < LT; ap += 4) red = fmaxf(red, Si[a * LT_LD1 + ap - 1] + Tt[ap * LT_LD1 + b]);
+        }
+        red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, 1));
+        red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, 2));
+        if (act && g == 0) {
+            float v = fmaxf(Tt[a * LT_LD1 + b], red);
+            if (j2 - i2 >= 4) {
+                // SW2 entry (i2+1, j2-1): in the tile, or in a finished tile below or to the left
+                const float sw = (a + 1 < LT && b >= 1) ? Tt[(a + 1) * LT_LD1 + b - 1]
+                                                        : Fc[(long long)(i2 + 1) * Np + (j2 - 1)];
+                v = fmaxf(v, sw + score_w(W.w, s2r[i2], s2r[j2]));
+            }
+            Tt[a * LT_LD1 + b] = v;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < LT * LT; e += 256) {
+        const int r = e >> 6, c = e & 63;
+        Fc[(long long)(LT * I + r) * Np + LT * J + c] = Tt[r * LT_LD1 + c];
+        FTc[(long long)(LT * J + r) * Np + LT * I + c] = Tt[c * LT_LD1 + r];
     }
 }
 
