@@ -11,8 +11,9 @@ terms with C(n) = n(n^2-1)/6, T(n) = n(n+1)/2 (twice this is the reference's "bp
 With N GPUs every rank fills its own pair (independent pairs, no collective): weak scaling; a batched
 workload is split over the ranks by estimated work instead (strong scaling), its scores gathered once.
 The default line also carries the sub-measurements of the other configurations (batched pairs/s,
-the balanced 256 x 256 pair, the forward + adjoint batch, the persistent fill against the graph of
-per-diagonal launches), bitwise windows of the benched tables
+the balanced 256 x 256 pair, the reference's own published shapes 16 x 750, 32 x 1024 and 32 x 3000,
+the forward + adjoint batch, the persistent fill against the graph of per-diagonal launches), bitwise
+windows of the benched tables
 against the reference's own fill ("parity"), and the reference's fill of a bounded sample timed on
 the host cores ("cpu_baseline").
 Prints ONE JSON line on rank 0.
@@ -395,6 +396,7 @@ def main_b200(args, world, rank, local):
     if not args.no_batched and single and args.workload == "single" and not args.pair and world == 1:
         extra["batched"] = measure_batched(eng)
         extra["balanced"] = measure_balanced(eng, peak, with_reference=not args.no_cpu_baseline)
+        extra["published_shapes"] = measure_published(eng, with_reference=not args.no_cpu_baseline)
         extra["grad"] = measure_grad(eng)
         extra["persistent"] = measure_persistent(local)
         eng.set_weights(wl.weights)
@@ -607,6 +609,39 @@ def measure_balanced(eng, peak, with_reference=True):
             except Exception as e:
                 d["parity"] = {"checked": False, "error": str(e)}
         out[tag] = d
+    return out
+
+
+# The reference's own published whole-fill shapes (short strand 1, long strand 2) and its published
+# times for them on 8 cores of a Xeon E-2278G (TPDS/experiments/bpmax_final.xlsx, sheet E2278G): a
+# different machine, reported beside the B200 time, not measured here. Each entry: (M, N, parity
+# prefix K of strand 1, reference N_tile, published ms).
+PUBLISHED_SHAPES = ((16, 750, 16, 64, 730.0), (32, 1024, 8, 64, 9710.0), (32, 3000, 0, 64, 188200.0))
+
+
+def measure_published(eng, with_reference=True):
+    """The reference's published shapes: B200 fill ms (median of two after a warm-up) and, where K > 0,
+    the reference's own fill of the strand-1 prefix pair compared bitwise with the same cells of the
+    GPU table (K = M: the whole table)."""
+    out = {"reference_published": "TPDS V3 whole fill, Xeon E-2278G, 8 cores (bpmax_final.xlsx)"}
+    for M, N, K, T, pub in PUBLISHED_SHAPES:
+        wl = W.single_pair(M, N, seed=6)
+        s1, s2 = wl.pairs[0]
+        eng.set_weights(wl.weights)
+        eng.score(s1, s2)  # warm-up (captures the graph)
+        ms = []
+        for _ in range(2):
+            eng.score(s1, s2)
+            ms.append(eng.last_timing()[0])
+        t = statistics.median(ms)
+        d = {"ms_per_fill": t, "value": wl.total_terms / (t * 1e-3) / 1e9, "unit": "Gterms/s",
+             "reference_published_ms": pub, "ratio_to_published": pub / t}
+        if with_reference and K > 0:
+            try:
+                d["parity"] = windows_vs_reference(eng, wl, K, 0, T)
+            except Exception as e:
+                d["parity"] = {"checked": False, "error": str(e)}
+        out[f"{M}x{N}"] = d
     return out
 
 
