@@ -625,17 +625,21 @@ def measure_published(eng, with_reference=True):
     GPU table (K = M: the whole table)."""
     out = {"reference_published": "TPDS V3 whole fill, Xeon E-2278G, 8 cores (bpmax_final.xlsx)"}
     for M, N, K, T, pub in PUBLISHED_SHAPES:
-        wl = W.single_pair(M, N, seed=6)
-        s1, s2 = wl.pairs[0]
-        eng.set_weights(wl.weights)
-        eng.score(s1, s2)  # warm-up (captures the graph)
-        ms = []
-        for _ in range(2):
-            eng.score(s1, s2)
-            ms.append(eng.last_timing()[0])
-        t = statistics.median(ms)
-        d = {"ms_per_fill": t, "value": wl.total_terms / (t * 1e-3) / 1e9, "unit": "Gterms/s",
-             "reference_published_ms": pub, "ratio_to_published": pub / t}
+        try:
+            wl = W.single_pair(M, N, seed=6)
+            s1, s2 = wl.pairs[0]
+            eng.set_weights(wl.weights)
+            eng.score(s1, s2)  # warm-up (captures the graph)
+            ms = []
+            for _ in range(2):
+                eng.score(s1, s2)
+                ms.append(eng.last_timing()[0])
+            t = statistics.median(ms)
+            d = {"ms_per_fill": t, "value": wl.total_terms / (t * 1e-3) / 1e9, "unit": "Gterms/s",
+                 "reference_published_ms": pub, "ratio_to_published": pub / t}
+        except Exception as e:  # reported, not fatal
+            out[f"{M}x{N}"] = {"error": str(e)}
+            continue
         if with_reference and K > 0:
             try:
                 d["parity"] = windows_vs_reference(eng, wl, K, 0, T)

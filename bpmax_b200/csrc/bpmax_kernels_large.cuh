@@ -544,7 +544,7 @@ s2_diag_kernel(const PairDesc *__restrict__ pairs, int p, const uint8_t *__restr
 
 // ------------------------------------------------------------------------------------------
 // Finalize for 64 < Np <= FIN_WIDE_MAX_NP (tables stored as tile images, bpmax_kernels.cuh): same
-// candidates and same results as finalize_large_kernel, with the inner wavefront pushed forward in
+// candidates and same results as the row-major tables' tile wavefront, pushed forward in
 // shared memory. The CTA keeps the cell's inner table diagonal-major and triangular,
 // D[e][i2] = F[i2][i2+e] (T(Np) floats), each open entry holding its running maximum. When inner
 // diagonal e is final, every open cell (e2 > e) takes its two candidates that read diagonal e,
