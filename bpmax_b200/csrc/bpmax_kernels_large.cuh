@@ -431,11 +431,22 @@ large_tile_local_kernel(const CellJob *__restrict__ jobs, const PairDesc *__rest
         const int a = l >= 0 ? slot : slot - l, b = a + l;  // entry slot of tile diagonal l
         const int i2 = LT * I + a, j2 = LT * J + b;
         const bool act = a < LT && b < LT && b >= 0 && i2 <= j2 && j2 < N;
-        float red = NEG_INF;
+        float red = NEG_INF, red1 = NEG_INF;  // two chains of maxima per thread
         if (act) {
-            for (int bp = g; bp < b; bp += 4) red = fmaxf(red, Tt[a * LT_LD1 + bp] + Sj[b * LT_LD1 + bp]);
-            for (int ap = a + 1 + g; ap < LT; ap += 4) red = fmaxf(red, Si[a * LT_LD1 + ap - 1] + Tt[ap * LT_LD1 + b]);
+            int bp = g;
+            for (; bp + 4 < b; bp += 8) {
+                red = fmaxf(red, Tt[a * LT_LD1 + bp] + Sj[b * LT_LD1 + bp]);
+                red1 = fmaxf(red1, Tt[a * LT_LD1 + bp + 4] + Sj[b * LT_LD1 + bp + 4]);
+            }
+            if (bp < b) red = fmaxf(red, Tt[a * LT_LD1 + bp] + Sj[b * LT_LD1 + bp]);
+            int ap = a + 1 + g;
+            for (; ap + 4 < LT; ap += 8) {
+                red = fmaxf(red, Si[a * LT_LD1 + ap - 1] + Tt[ap * LT_LD1 + b]);
+                red1 = fmaxf(red1, Si[a * LT_LD1 + ap + 3] + Tt[(ap + 4) * LT_LD1 + b]);
+            }
+            if (ap < LT) red = fmaxf(red, Si[a * LT_LD1 + ap - 1] + Tt[ap * LT_LD1 + b]);
         }
+        red = fmaxf(red, red1);
         red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, 1));
         red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, 2));
         if (act && g == 0) {
