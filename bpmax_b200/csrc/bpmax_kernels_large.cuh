@@ -394,7 +394,7 @@ large_tile_product_kernel(const CellJob *__restrict__ jobs, const PairDesc *__re
 // grid (NT - t) x cells, 256 threads: tile (I, I+t) of each outer cell, local coordinates
 // (a, b) = (i2 - 64I, j2 - 64J). An entry depends on the entries left of it in its tile row (R1),
 // below it in its tile column (R2) and at (a+1, b-1) (SW2), so the tile's diagonals b - a are done
-// in increasing order, one CTA barrier each, four threads per entry:
+// in increasing order, one CTA barrier each, 4 to 32 threads per entry:
 //   R1  T[a][b'] + S2(64J+b'+1, 64J+b),   b' < b     (ST1 block rows 64J+b, columns 64J+b')
 //   R2  S2(64I+a, 64I+a'-1) + T[a'][b],   a' > a     (S2M block rows 64I+a, columns 64I+a'-1)
 // (on a diagonal tile the terms outside b' >= a, a' <= b meet a -inf entry below the diagonal).
@@ -426,29 +426,32 @@ large_tile_local_kernel(const CellJob *__restrict__ jobs, const PairDesc *__rest
         Si[r * LT_LD1 + c] = S2M[(long long)(LT * I + r) * Np + LT * I + c];
     }
     __syncthreads();
-    const int g = tid & 3, slot = tid >> 2;  // four threads per entry, 64 entries per step
     for (int l = (t == 0 ? 1 : -(LT - 1)); l < LT; ++l) {
+        // the 64 - |l| entries of tile diagonal l, G threads each (G = 4 .. 32, as many as 256 allow):
+        // entries far from the tile's main diagonal hold the most terms and the fewest entries
+        const int E = LT - (l < 0 ? -l : l);
+        const int lg = E > 32 ? 2 : (E > 16 ? 3 : (E > 8 ? 4 : 5)), G = 1 << lg;
+        const int g = tid & (G - 1), slot = tid >> lg;
         const int a = l >= 0 ? slot : slot - l, b = a + l;  // entry slot of tile diagonal l
         const int i2 = LT * I + a, j2 = LT * J + b;
         const bool act = a < LT && b < LT && b >= 0 && i2 <= j2 && j2 < N;
         float red = NEG_INF, red1 = NEG_INF;  // two chains of maxima per thread
         if (act) {
             int bp = g;
-            for (; bp + 4 < b; bp += 8) {
+            for (; bp + G < b; bp += 2 * G) {
                 red = fmaxf(red, Tt[a * LT_LD1 + bp] + Sj[b * LT_LD1 + bp]);
-                red1 = fmaxf(red1, Tt[a * LT_LD1 + bp + 4] + Sj[b * LT_LD1 + bp + 4]);
+                red1 = fmaxf(red1, Tt[a * LT_LD1 + bp + G] + Sj[b * LT_LD1 + bp + G]);
             }
             if (bp < b) red = fmaxf(red, Tt[a * LT_LD1 + bp] + Sj[b * LT_LD1 + bp]);
             int ap = a + 1 + g;
-            for (; ap + 4 < LT; ap += 8) {
+            for (; ap + G < LT; ap += 2 * G) {
                 red = fmaxf(red, Si[a * LT_LD1 + ap - 1] + Tt[ap * LT_LD1 + b]);
-                red1 = fmaxf(red1, Si[a * LT_LD1 + ap + 3] + Tt[(ap + 4) * LT_LD1 + b]);
+                red1 = fmaxf(red1, Si[a * LT_LD1 + ap + G - 1] + Tt[(ap + G) * LT_LD1 + b]);
             }
             if (ap < LT) red = fmaxf(red, Si[a * LT_LD1 + ap - 1] + Tt[ap * LT_LD1 + b]);
         }
         red = fmaxf(red, red1);
-        red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, 1));
-        red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, 2));
+        for (int o = G >> 1; o > 0; o >>= 1) red = fmaxf(red, __shfl_xor_sync(0xffffffffu, red, o));  // G is CTA-uniform
         if (act && g == 0) {
             float v = fmaxf(Tt[a * LT_LD1 + b], red);
             if (j2 - i2 >= 4) {
