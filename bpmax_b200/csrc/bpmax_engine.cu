@@ -532,7 +532,7 @@ void launch_r0_wide(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaSt
 }
 
 // the finalize of one launch of cells wider than 64; returns the number of kernel launches
-int launch_fin_large(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaStream_t s)
+int launch_fin_large(bpmax_ctx *ctx, const Plan::Launch &L, cudaStream_t s)
 {
     const CellJob *jobs = (const CellJob *)ctx->celljobs.p + L.first;
     const CellJob *s1jobs = (const CellJob *)ctx->celljobs.p + L.s1_first;
@@ -547,7 +547,6 @@ int launch_fin_large(bpmax_ctx *ctx, const Plan &P, const Plan::Launch &L, cudaS
     }
     // row-major tables: start values, then per tile diagonal t the products over finished tiles and
     // the tiles' own wavefronts, then the SW1 pushes, the S1 slots and S1 of diagonal d+1
-    (void)P;
     float *FT = (float *)ctx->FT.p;
     const int nt32 = L.np / 32, NT = L.np / LT;
     int n = 0;
@@ -868,7 +867,7 @@ int enqueue_fill(bpmax_ctx *ctx, Plan &P, KernelProfile *kp = nullptr)
                     launch_r0only_fin(ctx, L, st);
                 } else {
                     switch (L.np > MAX_SMALL_NP ? 0 : L.np / 8) {
-                    case 0: launches += launch_fin_large(ctx, P, L, st) - 1; break;
+                    case 0: launches += launch_fin_large(ctx, L, st) - 1; break;
                     case 1: launch_fin<1>(ctx, L, st); break;
                     case 2: launch_fin<2>(ctx, L, st); break;
                     case 3: launch_fin<3>(ctx, L, st); break;
